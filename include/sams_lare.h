@@ -1,0 +1,117 @@
+/*
+ * sams_lare.h -- C ABI of the B200 LARE3D timestep.
+ *
+ * This is the drop-in boundary for the reference's LARE3D physics package
+ * (src/PhysicsPackages/LARE/shared_data.h:229-508).  In the reference the
+ * package is a C++ class driven by SAMS::runner events; here the same state
+ * and the same step are owned by an opaque solver handle whose memory lives
+ * on one GPU.  Plain pointers, sizes and status codes only: no C++ or torch
+ * types cross this boundary.  Host buffers use the box layout of
+ * sams_lare_layout.h.
+ *
+ * Every function returns SAMS_OK (0) or a negative status; the message of
+ * the last failure on the calling thread is available from
+ * sams_lare_last_error().  Calls on one handle are not thread-safe.
+ */
+#ifndef SAMS_LARE_H
+#define SAMS_LARE_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "sams_lare_layout.h"
+#include "sams_lare_ic.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum sams_status {
+    SAMS_OK = 0,
+    SAMS_ERR_INVALID = -1,      /* bad argument or unsupported option      */
+    SAMS_ERR_NOMEM = -2,        /* device or host allocation failed         */
+    SAMS_ERR_CUDA = -3,         /* a CUDA runtime call failed               */
+    SAMS_ERR_UNSUPPORTED = -4,  /* geometry / rke / custom BC not built     */
+    SAMS_ERR_NONFINITE = -5,    /* the timestep became NaN or infinite      */
+    SAMS_ERR_TIMEOUT = -6,      /* a bounded wait ran out                   */
+    SAMS_ERR_BUDGET = -7        /* request exceeds the memory budget        */
+};
+
+typedef struct sams_lare_solver sams_lare_solver;
+
+/* Version of this ABI (major * 100 + minor). */
+int sams_lare_abi_version(void);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *sams_lare_last_error(void);
+
+/* Create a solver on a CUDA device: allocates the 13 harness variables and
+ * the step's scratch on that device and builds the grid metrics.
+ * Replaces LARE3D::registerAxes/registerVariables/allocate/grid
+ * (setup.cpp:27-437) and the runner's decomposeAndAllocate
+ * (include/runner/runner.h:456-464).  Boundary conditions are copied; they
+ * replace the IC package's setBoundaryConditions
+ * (variableDef::addBoundaryCondition, include/harness/variableDef.h:402-481).
+ * Supported: Cartesian geometry, rke = 0. */
+int sams_lare_create(const sams_lare_params *params, const sams_lare_bcs *bcs,
+                     int device, sams_lare_solver **out);
+
+/* Free all device memory of the solver. */
+int sams_lare_destroy(sams_lare_solver *h);
+
+/* Run the solver's work on this CUDA stream (cudaStream_t passed as void*);
+ * NULL selects the solver's own stream. */
+int sams_lare_set_stream(sams_lare_solver *h, void *stream);
+
+/* Replace one (field, dim, edge) boundary condition; see sams_lare_bc_kind.
+ * Replaces variableDef::addBoundaryCondition(dim, edge, bc). */
+int sams_lare_set_bc(sams_lare_solver *h, int field, int dim, int edge,
+                     int kind, double value);
+
+/* Copy one field from a host box buffer to the device (asynchronous on the
+ * solver's stream when the buffer is pinned).  Together they replace the IC
+ * package's initialConditions writes into variableRegistry arrays
+ * (src/InitialConditions/OrszagTang/OrszagTang.cpp:104-156). */
+int sams_lare_upload_field(sams_lare_solver *h, int field, const double *host_box);
+int sams_lare_download_field(sams_lare_solver *h, int field, double *host_box);
+
+/* Same, from / to a device box buffer (e.g. a CUDA tensor's storage). */
+int sams_lare_upload_field_device(sams_lare_solver *h, int field, const double *dev_box);
+int sams_lare_download_field_device(sams_lare_solver *h, int field, double *dev_box);
+
+/* Advance nsteps full timesteps, asynchronously on the solver's stream.
+ * One step is the runner's startOfTimestep -> halfTimestep -> step/time
+ * update -> endOfTimestep sequence (include/runner/runner.h:564-586) over
+ * LARE3D::lagrangian_step, corrector_step and eulerian_remap
+ * (shared_data.h:397-419).  The CFL timestep is reduced on the device
+ * (lagran.cpp:380-443) and never read back. */
+int sams_lare_step(sams_lare_solver *h, int64_t nsteps);
+
+/* Same, but the nsteps are recorded once into a CUDA graph and replayed. */
+int sams_lare_step_graph(sams_lare_solver *h, int64_t nsteps);
+
+/* Wait for the solver's stream. */
+int sams_lare_synchronize(sams_lare_solver *h);
+
+/* Current dt / time / step count (these synchronise).  Replace
+ * SAMS::timeState (runner.h:20-25) and LARE3D::getTimestep. */
+int sams_lare_get_dt(sams_lare_solver *h, double *dt);
+int sams_lare_get_time(sams_lare_solver *h, double *time);
+int sams_lare_get_step(sams_lare_solver *h, int64_t *step);
+
+/* Device address of a field's box storage and its element strides
+ * (x, y, z; z stride is 1) and z offset: element (i,j,k) lives at
+ * ptr[(i+2)*sx + (j+2)*sy + (k+zoff)]. */
+int sams_lare_field_device_ptr(sams_lare_solver *h, int field, double **ptr,
+                               int64_t strides[3], int64_t *zoff);
+
+/* Device bytes held by the solver. */
+int sams_lare_device_bytes(sams_lare_solver *h, int64_t *bytes);
+
+/* Number of kernel launches one sams_lare_step(h, 1) issues. */
+int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SAMS_LARE_H */

@@ -1,0 +1,177 @@
+// lare_capi.cu -- the extern "C" boundary (include/sams_lare.h) over
+// sams::Solver.
+#include "sams_lare.h"
+#include "lare_solver.cuh"
+
+#include <cstring>
+#include <new>
+#include <string>
+
+struct sams_lare_solver {
+    sams::Solver s;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int rc, const std::string &msg)
+{
+    g_last_error = msg;
+    return rc;
+}
+
+int pass(sams_lare_solver *h, int rc)
+{
+    if (rc != SAMS_OK) g_last_error = h->s.err;
+    return rc;
+}
+
+cudaMemcpyKind host_kind(const void *p)
+{
+    // pageable and pinned host memory both work with cudaMemcpyDefault
+    (void)p;
+    return cudaMemcpyDefault;
+}
+}  // namespace
+
+extern "C" {
+
+int sams_lare_abi_version(void) { return 100; }
+
+const char *sams_lare_last_error(void) { return g_last_error.c_str(); }
+
+int sams_lare_create(const sams_lare_params *params, const sams_lare_bcs *bcs, int device, sams_lare_solver **out)
+{
+    if (!params || !bcs || !out) return fail(SAMS_ERR_INVALID, "sams_lare_create: null argument");
+    *out = nullptr;
+    sams_lare_solver *h = new (std::nothrow) sams_lare_solver();
+    if (!h) return fail(SAMS_ERR_NOMEM, "sams_lare_create: host allocation failed");
+    int rc = h->s.init(*params, *bcs, device);
+    if (rc != SAMS_OK) {
+        g_last_error = h->s.err;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return SAMS_OK;
+}
+
+int sams_lare_destroy(sams_lare_solver *h)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "sams_lare_destroy: null handle");
+    delete h;
+    return SAMS_OK;
+}
+
+int sams_lare_set_stream(sams_lare_solver *h, void *stream)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.set_stream(static_cast<cudaStream_t>(stream)));
+}
+
+int sams_lare_set_bc(sams_lare_solver *h, int field, int dim, int edge, int kind, double value)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.set_bc(field, dim, edge, kind, value));
+}
+
+int sams_lare_upload_field(sams_lare_solver *h, int field, const double *host_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.upload(field, host_box, host_kind(host_box)));
+}
+
+int sams_lare_download_field(sams_lare_solver *h, int field, double *host_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.download(field, host_box, host_kind(host_box)));
+}
+
+int sams_lare_upload_field_device(sams_lare_solver *h, int field, const double *dev_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.upload(field, dev_box, cudaMemcpyDeviceToDevice));
+}
+
+int sams_lare_download_field_device(sams_lare_solver *h, int field, double *dev_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.download(field, dev_box, cudaMemcpyDeviceToDevice));
+}
+
+int sams_lare_step(sams_lare_solver *h, int64_t nsteps)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.step(nsteps));
+}
+
+int sams_lare_step_graph(sams_lare_solver *h, int64_t nsteps)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.step_graph(nsteps));
+}
+
+int sams_lare_synchronize(sams_lare_solver *h)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null handle");
+    return pass(h, h->s.sync());
+}
+
+int sams_lare_get_dt(sams_lare_solver *h, double *dt)
+{
+    if (!h || !dt) return fail(SAMS_ERR_INVALID, "null argument");
+    sams::Scalars s;
+    int rc = h->s.scalars(s);
+    if (rc) return pass(h, rc);
+    *dt = s.dt;
+    return SAMS_OK;
+}
+
+int sams_lare_get_time(sams_lare_solver *h, double *time)
+{
+    if (!h || !time) return fail(SAMS_ERR_INVALID, "null argument");
+    sams::Scalars s;
+    int rc = h->s.scalars(s);
+    if (rc) return pass(h, rc);
+    *time = s.time;
+    return SAMS_OK;
+}
+
+int sams_lare_get_step(sams_lare_solver *h, int64_t *step)
+{
+    if (!h || !step) return fail(SAMS_ERR_INVALID, "null argument");
+    sams::Scalars s;
+    int rc = h->s.scalars(s);
+    if (rc) return pass(h, rc);
+    *step = s.step;
+    return SAMS_OK;
+}
+
+int sams_lare_field_device_ptr(sams_lare_solver *h, int field, double **ptr, int64_t strides[3], int64_t *zoff)
+{
+    if (!h || !ptr || !strides || !zoff || field < 0 || field >= SAMS_NFIELDS)
+        return fail(SAMS_ERR_INVALID, "invalid argument");
+    const sams::Geom &g = h->s.geom();
+    *ptr = h->s.field_ptr(field);
+    strides[0] = g.sx;
+    strides[1] = g.sy;
+    strides[2] = 1;
+    *zoff = g.zoff;
+    return SAMS_OK;
+}
+
+int sams_lare_device_bytes(sams_lare_solver *h, int64_t *bytes)
+{
+    if (!h || !bytes) return fail(SAMS_ERR_INVALID, "invalid argument");
+    *bytes = h->s.device_bytes();
+    return SAMS_OK;
+}
+
+int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches)
+{
+    if (!h || !launches) return fail(SAMS_ERR_INVALID, "invalid argument");
+    *launches = h->s.launches_per_step();
+    return SAMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,261 @@
+// lare_device.cuh -- device-side data layout and point formulas of the
+// LARE3D timestep on B200.
+//
+// Layout: every field is one "box" over indices -2..n+2 per dimension, z
+// fastest, with the z row padded so that interior index k = 1 starts on a
+// 32-byte boundary (zoff = 3) and rows are a multiple of 8 doubles.  All
+// fields share one geometry, so one offset serves every array.
+//
+// Arithmetic: this translation unit is compiled with --fmad=false and the
+// formulas below keep the reference's evaluation order term by term
+// (left-to-right sums, the same parenthesisation), so results are identical
+// to the reference CPU build with -ffp-contract=off.  Double division and
+// sqrt are IEEE round-to-nearest on the GPU as on the CPU.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "sams_lare_layout.h"
+
+namespace sams {
+
+struct Geom {
+    int nx, ny, nz;
+    long long sx, sy;  // element strides of i and j (k stride is 1)
+    int zoff;          // k + zoff is the position of index k in its row
+    long long nelem;   // doubles per field allocation
+};
+
+// Host/device helpers for the box geometry.
+__host__ __device__ inline long long box_off(const Geom &g, int i, int j, int k)
+{
+    return (long long)(i + 2) * g.sx + (long long)(j + 2) * g.sy + (long long)(k + g.zoff);
+}
+
+// Staggering of a field in one dimension (1 = half cell), the device-side
+// copy of sams_lare_field_stagger.
+__host__ __device__ constexpr int field_half(int f, int d)
+{
+    return (f >= SAMS_F_VX && f <= SAMS_F_VZ1) ? 1
+           : (f == SAMS_F_BX) ? (d == 0)
+           : (f == SAMS_F_BY) ? (d == 1)
+           : (f == SAMS_F_BZ) ? (d == 2)
+           : 0;
+}
+
+// 1-D axes (index i at [i + 2]); Cartesian metrics are products of these.
+struct Axes {
+    const double *dxb, *dyb, *dzb, *dxc, *dyc, *dzc;
+};
+
+struct Phys {
+    double gamma, mu0, visc1, visc2_norm, dt_multiplier, eta_bg, eta0, j_max;
+};
+
+// Per-solve device scalars.
+struct Scalars {
+    double dt;        // timestep of the step in progress (previous step's
+                      // value until the CFL reduction has run)
+    double dtr;       // LARE's dtr (equals the reduced dt)
+    double dt_sub;    // resistive sub-step
+    double time;      // simulation time
+    unsigned long long dtmin_bits;  // running min of the CFL candidates
+    long long step;
+    int nsub;         // resistive sub-steps this step
+    int status;       // 0 ok, nonzero: non-finite dt seen
+};
+
+// LARE uses the same 32 arrays for every solve: the 13 harness variables and
+// 19 scratch arrays whose roles change with the phase of the step.
+enum ScratchId {
+    // Lagrangian phase
+    S_CS = 0, S_RHOV, S_CSV, S_A1, S_A2, S_A3, S_VH, S_FXV, S_FYV, S_FZV,
+    S_CV1, S_B1X, S_B1Y, S_B1Z, S_PE, S_PI, S_FX, S_FY, S_FZ,
+    NSCRATCH
+};
+// Resistive sub-step aliases (live between the CFL reduction and the
+// predictor, when cs, cs_v, cv1 and fx are free; pe holds the cell
+// electron pressure from before the Ohmic heating).
+#define S_FLUXX S_CS
+#define S_FLUXY S_CSV
+#define S_FLUXZ S_CV1
+#define S_CURLB S_FX
+// Remap aliases (the whole Lagrangian scratch is dead by then).
+#define S_R_CV1 S_CV1
+#define S_R_CV2 S_CS
+#define S_R_DB1 S_RHOV
+#define S_R_RHO1 S_CSV
+#define S_R_CVC1 S_A1
+#define S_R_CT1 S_A2
+#define S_R_CT2 S_A3
+#define S_R_FE1 S_VH
+#define S_R_FE2 S_FXV
+#define S_R_RVN S_FYV
+#define S_R_CV2N S_FZV
+#define S_R_DMN S_B1X
+#define S_R_V1S S_B1Y
+#define S_R_FM1 S_B1Z
+#define S_R_FM2 S_PE
+#define S_R_FM3 S_PI
+
+struct Ctx {
+    Geom g;
+    Axes ax;
+    Phys p;
+    double *f[13];
+    double *s[NSCRATCH];
+    Scalars *sc;
+};
+
+namespace dev {
+
+constexpr double NONE_ZERO = DBL_EPSILON;  // LARE simulationData::none_zero
+constexpr double SIXTH = 1.0 / 6.0;
+
+// portableWrapper min/max semantics (include/pp/utils.h:277-335).
+__device__ __forceinline__ double pmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double pmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double pmin_list3(double a, double b, double c)
+{
+    double m = a;
+    if (b < m) m = b;
+    if (c < m) m = c;
+    return m;
+}
+__device__ __forceinline__ double pmin_list4(double a, double b, double c, double d)
+{
+    double m = a;
+    if (b < m) m = b;
+    if (c < m) m = c;
+    if (d < m) m = d;
+    return m;
+}
+
+// Da, ss and Di of the van Leer limiter written in every remap flux function
+// (e.g. xremap.cpp:309-314).
+__device__ __forceinline__ double limiter_Di(double sign_v, double phi, double dfi, double dfu,
+                                             double dxci, double dxcu, double dxbu)
+{
+    double Da = (2.0 - phi) * fabs(dfi) / dxci + (1.0 + phi) * fabs(dfu) / dxcu;
+    Da = Da * SIXTH;
+    double ss = 0.5 * ((dfi >= 0.0 ? 1.0 : -1.0) + (dfu >= 0.0 ? 1.0 : -1.0));
+    return sign_v * ss * pmin_list3(fabs(Da) * dxbu, fabs(dfi), fabs(dfu));
+}
+
+// Evans-Hawley constrained-transport flux of a transverse face field
+// (vx_by_flux xremap.cpp:269-319 and the five analogues in x/y/zremap.cpp).
+__device__ __forceinline__ double ct_flux(double v_advect, double dt, double bm, double bi, double bp,
+                                          double bp2, double dbm, double dbi, double dbp, double dbp2,
+                                          double dci, double dcm, double dcp, double cv1i, double cv1p)
+{
+    double o_v = v_advect * dt;
+    double fm = bm / dbm, fi = bi / dbi, fp = bp / dbp, fp2 = bp2 / dbp2;
+    double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    double sign_v = (v_advect >= 0.0) ? 1.0 : -1.0;
+    double vad_p = (sign_v + 1.0) * 0.5;
+    double vad_m = 1.0 - vad_p;
+    double fu = fi * vad_p + fp * vad_m;
+    double dfu = dfm * vad_p + dfp * vad_m;
+    double dxcu = dcm * vad_p + dcp * vad_m;
+    double dxbu = cv1i * vad_p + cv1p * vad_m;
+    double dxu = dbi * vad_p + dbp * vad_m;
+    double phi = fabs(o_v) / dxu;
+    double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
+    return (fu + Di * (1.0 - phi)) * o_v;
+}
+
+// Mass flux through a face (x_mass_flux xremap.cpp:373-422 and analogues).
+__device__ __forceinline__ double mass_flux(double v_advect, double dt, double area, double fm, double fi,
+                                            double fp, double fp2, double dci, double dcm, double dcp,
+                                            double cv1i, double cv1p)
+{
+    double o_v = v_advect * dt * area;
+    double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    double sign_v = (v_advect >= 0.0) ? 1.0 : -1.0;
+    double vad_p = (sign_v + 1.0) * 0.5;
+    double vad_m = 1.0 - vad_p;
+    double fu = fi * vad_p + fp * vad_m;
+    double dfu = dfm * vad_p + dfp * vad_m;
+    double dxcu = dcm * vad_p + dcp * vad_m;
+    double dxbu = cv1i * vad_p + cv1p * vad_m;
+    double phi = fabs(o_v) / dxbu;
+    double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
+    return (fu + Di * (1.0 - phi)) * o_v;
+}
+
+// Specific-energy flux (x_energy_flux xremap.cpp:429-483 and analogues).
+__device__ __forceinline__ double energy_flux(double v_advect, double dt, double area, double fm, double fi,
+                                              double fp, double fp2, double dci, double dcm, double dcp,
+                                              double cv1i, double cv1p, double rho1i, double rho1p, double dm)
+{
+    double o_v = v_advect * dt * area;
+    double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    double sign_v = (v_advect >= 0.0) ? 1.0 : -1.0;
+    double vad_p = (sign_v + 1.0) * 0.5;
+    double vad_m = 1.0 - vad_p;
+    double fu = fi * vad_p + fp * vad_m;
+    double dfu = dfm * vad_p + dfp * vad_m;
+    double dxcu = dcm * vad_p + dcp * vad_m;
+    double dxbu = cv1i * vad_p + cv1p * vad_m;
+    double phi = fabs(o_v) / dxbu;
+    double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
+    double rhou = rho1i * vad_p + rho1p * vad_m;
+    double dmu = fabs(dm) / dxbu / rhou;
+    return (fu + Di * (1.0 - dmu)) * dm;
+}
+
+// Momentum flux times dm (x_mom_flux xremap.cpp:485-566 and analogues;
+// the z sweep divides |dm| by (dzbu * rhou) in one step, zremap.cpp:509).
+template <bool ZFORM>
+__device__ __forceinline__ double mom_flux_dm(double v_advect, double dt, double area, double fm, double fi,
+                                              double fp, double fp2, double dci, double dcm, double dcp,
+                                              double cvci, double cvcp, double rvi, double rvp, double dm)
+{
+    double o_v = v_advect * dt * area;
+    double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    double sign_v = (o_v >= 0.0) ? 1.0 : -1.0;
+    double vad_p = (sign_v + 1.0) * 0.5;
+    double vad_m = 1.0 - vad_p;
+    double fu = fi * vad_p + fp * vad_m;
+    double dfu = dfm * vad_p + dfp * vad_m;
+    double dxcu = dcm * vad_p + dcp * vad_m;
+    double dxbu = cvci * vad_p + cvcp * vad_m;
+    double phi = fabs(o_v) / dxbu;
+    double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
+    double rhou = rvi * vad_p + rvp * vad_m;
+    double dmu = ZFORM ? fabs(dm) / (dxbu * rhou) : fabs(dm) / dxbu / rhou;
+    double flux = fu + Di * (1.0 - dmu);
+    return flux * dm;
+}
+
+// Caramana edge viscosity (lagran.cpp:56-93).  v[a] are the four points
+// along the edge direction, o1/o2 the edge ends.
+__device__ __forceinline__ double edge_viscosity(double dt, double visc1, double v2n, const double *vx,
+                                                 const double *vy, const double *vz, const double *rho_v,
+                                                 double dvdots, double dx, double dxm, double dxp,
+                                                 double cs_edge, long long o0, long long o1, long long o2,
+                                                 long long o3)
+{
+    dvdots = pmin(0.0, dvdots);
+    double rv1 = rho_v[o1], rv2 = rho_v[o2];
+    double rho_edge = 2.0 * rv1 * rv2 / (rv1 + rv2);
+    double vx1 = vx[o1], vx2 = vx[o2], vy1 = vy[o1], vy2 = vy[o2], vz1 = vz[o1], vz2 = vz[o2];
+    double dvx = vx1 - vx2, dvy = vy1 - vy2, dvz = vz1 - vz2;
+    double dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+    double dv = sqrt(dv2);
+    bool small = dv * dt / dx < 1.e-14;
+    dvdots = small ? 0.0 : dvdots / dv;
+    double dvxm = vx[o0] - vx1, dvxp = vx2 - vx[o3];
+    double dvym = vy[o0] - vy1, dvyp = vy2 - vy[o3];
+    double dvzm = vz[o0] - vz1, dvzp = vz2 - vz[o3];
+    double rl = small ? 1.0 : (dvxp * dvx + dvyp * dvy + dvzp * dvz) * dx / (dxp * dv2);
+    double rr = small ? 1.0 : (dvxm * dvx + dvym * dvy + dvzm * dvz) * dx / (dxm * dv2);
+    double psi = pmin_list4(0.5 * (rr + rl), 2.0 * rl, 2.0 * rr, 1.0);
+    psi = pmax(0.0, psi);
+    double q_k_bar = rho_edge * (v2n * dv + sqrt(v2n * v2n * dv2 + (visc1 * cs_edge) * (visc1 * cs_edge)));
+    return q_k_bar * (1.0 - psi) * dvdots;
+}
+
+}  // namespace dev
+}  // namespace sams

@@ -1,0 +1,991 @@
+// lare_ops.cuh -- the fused phases of one LARE3D timestep as per-point
+// device operations.  Each Op has
+//   bounds(g, arg, lo, hi)   the index box the phase covers, and
+//   run(c, arg, i, j, k)     the work of one (i, j, k) of that box,
+// so the same code runs under the single-solve launcher (one grid per
+// phase) and the batched launcher (one grid over a worklist of tiles from
+// many solves).
+//
+// Fusion plan (reference kernels each op replaces in brackets):
+//   CellPrep   cs                                  [lagran.cpp:113-125, 192-198]
+//   NodePrep   rho_v, cs_v                         [lagran.cpp:128-153, 201-215]
+//   Alpha      alpha1..3                           [lagran.cpp:218-279]
+//   Visc       visc_heat, f*_visc, CFL candidate   [lagran.cpp:284-376, 388-439]
+//   ResistRK   eta (on the fly), edge E, curlb     [lagran.cpp:449-474, 511-533]
+//   ResistB    B update, Ohmic heating, b1 copy    [lagran.cpp:482-499, 541-587]
+//   Pred1      cv1, half-step B*cv1, p_e/p_i       [lagran.cpp:598-614, 810-880]
+//   Pred2      forces, v1                          [lagran.cpp:619-733]
+//   Corr1      shock heating                       [lagran.cpp:888-992]
+//   Corr2      velocity, energies, density         [lagran.cpp:754-798]
+//   BScale / BUnscale  B <-> flux form             [remap.cpp:46-50, 91-95]
+//   SweepVol   cv1, cv2, db1, rho1, dm = 0         [xremap.cpp:24-70 + y/z]
+//   SweepCvc   cvc1                                [xremap.cpp:74-81]
+//   SweepCT    both CT fluxes                      [xremap.cpp:269-371]
+//   SweepCTUpd both CT updates                     [xremap.cpp:87-115]
+//   SweepMass  dm                                  [xremap.cpp:373-422]
+//   SweepS6    rho, energy fluxes, vertex rho_v,   [xremap.cpp:121-221]
+//              cv2 (node), dm (node), v1 shift
+//   SweepS7    energy updates, momentum fluxes*dm  [xremap.cpp:130-152, 485-566]
+//   SweepS8    momentum updates (rho_v1 inline)    [xremap.cpp:226-261]
+// Metric arrays (cv, dxab, ...) are products of the 1-D spacings in
+// Cartesian geometry (setup.cpp:337-390) and are formed on the fly in the
+// same multiplication order.
+#pragma once
+
+#include "lare_device.cuh"
+#include "sams_lare_layout.h"
+
+namespace sams {
+namespace ops {
+
+using namespace dev;
+
+#define LOFF(i, j, k) box_off(g, (i), (j), (k))
+
+__device__ __forceinline__ double cv_at(const Ctx &c, int i, int j, int k)
+{
+    return c.ax.dxb[i + 2] * (c.ax.dyb[j + 2] * c.ax.dzb[k + 2]);
+}
+__device__ __forceinline__ double dxab_at(const Ctx &c, int i, int j, int k)
+{
+    (void)i;
+    return c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
+}
+__device__ __forceinline__ double dyab_at(const Ctx &c, int i, int j, int k)
+{
+    (void)j;
+    return c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
+}
+__device__ __forceinline__ double dzab_at(const Ctx &c, int i, int j, int k)
+{
+    (void)k;
+    return c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
+}
+__device__ __forceinline__ double dxac_at(const Ctx &c, int i, int j, int k)
+{
+    (void)i;
+    return c.ax.dyb[j + 2] * c.ax.dzc[k + 2];
+}
+__device__ __forceinline__ double dyac_at(const Ctx &c, int i, int j, int k)
+{
+    (void)j;
+    return c.ax.dxb[i + 2] * c.ax.dzc[k + 2];
+}
+__device__ __forceinline__ double cvc_at(const Ctx &c, int i, int j, int k)
+{
+    return c.ax.dxb[i + 2] * (c.ax.dyb[j + 2] * c.ax.dzc[k + 2]);
+}
+
+__host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int a1, int b1, int a2, int b2)
+{
+    lo[0] = a0; hi[0] = b0;
+    lo[1] = a1; hi[1] = b1;
+    lo[2] = a2; hi[2] = b2;
+}
+
+// ---------------------------------------------------------------------------
+// Lagrangian phase
+// ---------------------------------------------------------------------------
+
+// Sound speed on cells; with resistive MHD also keeps p_e, which the
+// predictor needs from before the Ohmic heating (lagran.cpp:121, 606).
+struct CellPrep {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long o = LOFF(i, j, k);
+        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        double bx1 = 0.5 * (bx[o] + bx[o - g.sx]);
+        double by1 = 0.5 * (by[o] + by[o - g.sy]);
+        double bz1 = 0.5 * (bz[o] + bz[o - 1]);
+        const double gm = c.p.gamma;
+        double rho = c.f[SAMS_F_RHO][o];
+        double pe = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ELECTRON][o];
+        double pi = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ION][o];
+        double p = pe + pi;
+        double rmin = pmax(rho, NONE_ZERO);
+        double b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
+        c.s[S_CS][o] = sqrt((gm * p + b2) / rmin);
+        if (resistive) c.s[S_PE][o] = pe;
+    }
+};
+
+// Node density and sound speed (8-cell volume-weighted averages).
+struct NodePrep {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const double *rho = c.f[SAMS_F_RHO], *cs = c.s[S_CS];
+        const int ip = i + 1, jp = j + 1, kp = k + 1;
+        double cv0 = cv_at(c, i, j, k), cv1 = cv_at(c, ip, j, k), cv2 = cv_at(c, i, jp, k), cv3 = cv_at(c, ip, jp, k);
+        double cv4 = cv_at(c, i, j, kp), cv5 = cv_at(c, ip, j, kp), cv6 = cv_at(c, i, jp, kp), cv7 = cv_at(c, ip, jp, kp);
+        long long o0 = LOFF(i, j, k), o1 = LOFF(ip, j, k), o2 = LOFF(i, jp, k), o3 = LOFF(ip, jp, k);
+        long long o4 = LOFF(i, j, kp), o5 = LOFF(ip, j, kp), o6 = LOFF(i, jp, kp), o7 = LOFF(ip, jp, kp);
+        double sum_rho_cv = rho[o0] * cv0 + rho[o1] * cv1 + rho[o2] * cv2 + rho[o3] * cv3 +
+                            rho[o4] * cv4 + rho[o5] * cv5 + rho[o6] * cv6 + rho[o7] * cv7;
+        double sum_cv = cv0 + cv1 + cv2 + cv3 + cv4 + cv5 + cv6 + cv7;
+        c.s[S_RHOV][o0] = sum_rho_cv / sum_cv;
+        double cv_v = 0.125 * sum_cv;
+        double sum = cs[o0] * cv0 + cs[o1] * cv1 + cs[o2] * cv2 + cs[o3] * cv3 +
+                     cs[o4] * cv4 + cs[o5] * cv5 + cs[o6] * cv6 + cs[o7] * cv7;
+        c.s[S_CSV][o0] = 0.125 * sum / cv_v;
+    }
+};
+
+// Edge viscosities.  dt is the previous step's (the CFL reduction of this
+// step runs later, lagran.cpp:155-156).
+struct Alpha {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+        const double *rho_v = c.s[S_RHOV], *cs_v = c.s[S_CSV];
+        const double dt = c.sc->dt, visc1 = c.p.visc1, v2n = c.p.visc2_norm;
+        const long long o = LOFF(i, j, k);
+        if (i >= 0 && j >= 0) {  // alpha1: (0..nx+1, 0..ny+2, 0..nz+2)
+            long long o1 = LOFF(i - 1, j - 1, k - 1), o2 = LOFF(i, j - 1, k - 1);
+            long long o0 = o1 - g.sx, o3 = o2 + g.sx;
+            double dx = c.ax.dxb[i + 2], dxp = c.ax.dxb[i + 3], dxm = c.ax.dxb[i + 1];
+            double dvdots = -(vx[o1] - vx[o2]);
+            double cs_edge = pmin(cs_v[o1], cs_v[o2]);
+            c.s[S_A1][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+        }
+        if (j >= 0 && j <= g.ny + 1) {  // alpha2: (-1..nx+1, 0..ny+1, 0..nz+2)
+            long long o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
+            long long o0 = o1 - g.sy, o3 = o2 + g.sy;
+            double dx = c.ax.dyb[j + 2], dxp = c.ax.dyb[j + 3], dxm = c.ax.dyb[j + 1];
+            double dvdots = -(vy[o1] - vy[o2]);
+            double cs_edge = pmin(cs_v[o1], cs_v[o2]);
+            c.s[S_A2][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+        }
+        if (j <= g.ny + 1 && k <= g.nz + 1) {  // alpha3: (-1..nx+1, -1..ny+1, 0..nz+1)
+            long long o1 = o - 1, o2 = o;
+            long long o0 = o1 - 1, o3 = o2 + 1;
+            double dx = c.ax.dzb[k + 2], dxp = c.ax.dzb[k + 3], dxm = c.ax.dzb[k + 1];
+            double dvdots = -(vz[o1] - vz[o2]);
+            double cs_edge = pmin(cs_v[o1], cs_v[o2]);
+            c.s[S_A3][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+        }
+    }
+};
+
+// Viscous pressure and heating on cells, viscous forces on nodes and the
+// cell's CFL candidate (p_visc is consumed here and never stored).
+// Returns the candidate (DBL_MAX outside the CFL range).
+struct Visc {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
+    }
+    __device__ static double run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+        const double *a1a = c.s[S_A1], *a2a = c.s[S_A2], *a3a = c.s[S_A3];
+        const long long SX = g.sx, SY = g.sy;
+        const long long o = LOFF(i, j, k);
+        const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
+#define DV2(a, b) ((vx[a] - vx[b]) * (vx[a] - vx[b]) + (vy[a] - vy[b]) * (vy[a] - vy[b]) + (vz[a] - vz[b]) * (vz[a] - vz[b]))
+        // cell (ix, iy, iz) corners: m = minus one along that axis
+        const long long c_mmm = o - SX - SY - 1, c_0mm = o - SY - 1, c_00m = o - 1, c_m0m = o - SX - 1;
+        const long long c_mm0 = o - SX - SY, c_0m0 = o - SY, c_000 = o, c_m00 = o - SX;
+        double a1 = DV2(c_mmm, c_0mm);
+        double a2 = DV2(c_0mm, c_00m);
+        double a3 = DV2(c_00m, c_m0m);
+        double a4 = DV2(c_m0m, c_mmm);
+        double a5 = DV2(c_mm0, c_0m0);
+        double a6 = DV2(c_0m0, c_000);
+        double a7 = DV2(c_000, c_m00);
+        double a8 = DV2(c_m00, c_mm0);
+        double a9 = DV2(c_00m, c_000);
+        double a10 = DV2(c_m0m, c_m00);
+        double a11 = DV2(c_mmm, c_mm0);
+        double a12 = DV2(c_0mm, c_0m0);
+#undef DV2
+        double p_visc = 0.0;
+        p_visc = pmax(p_visc, -a1a[o] * sqrt(a1));
+        p_visc = pmax(p_visc, -a2a[o] * sqrt(a2));
+        p_visc = pmax(p_visc, -a3a[o] * sqrt(a9));
+        double vh = -0.25 * dy * dz * a1a[o] * a1
+                    - 0.25 * dx * dz * a2a[o] * a2
+                    - 0.25 * dy * dz * a1a[o + SY] * a3
+                    - 0.25 * dx * dz * a2a[o - SX] * a4
+                    - 0.25 * dy * dz * a1a[o + 1] * a5
+                    - 0.25 * dx * dz * a2a[o + 1] * a6
+                    - 0.25 * dy * dz * a1a[o + SY + 1] * a7
+                    - 0.25 * dx * dz * a2a[o - SX + 1] * a8
+                    - 0.25 * dx * dy * a3a[o] * a9
+                    - 0.25 * dx * dy * a3a[o - SX] * a10
+                    - 0.25 * dx * dy * a3a[o - SX - SY] * a11
+                    - 0.25 * dx * dy * a3a[o - SY] * a12;
+        const double cv = dx * (dy * dz);
+        c.s[S_VH][o] = vh / cv;
+        if (i > g.nx || j > g.ny || k > g.nz) return DBL_MAX;
+
+        // viscous forces on node (i, j, k)
+        {
+            double e1 = a1a[o + SY + 1] * dy * dz;
+            double e2 = a1a[o + SX + SY + 1] * dy * dz;
+            double e3 = a2a[o + 1] * dx * dz;
+            double e4 = a2a[o + SY + 1] * dx * dz;
+            double e5 = a3a[o] * dx * dy;
+            double e6 = a3a[o + 1] * dx * dy;
+            // cv_v = 0.125 * (8-cell sum of cv) (lagran.cpp:142-151)
+            const int ip = i + 1, jp = j + 1, kp = k + 1;
+            double sum_cv = cv_at(c, i, j, k) + cv_at(c, ip, j, k) + cv_at(c, i, jp, k) + cv_at(c, ip, jp, k) +
+                            cv_at(c, i, j, kp) + cv_at(c, ip, j, kp) + cv_at(c, i, jp, kp) + cv_at(c, ip, jp, kp);
+            double cv_v = 0.125 * sum_cv;
+#define FV(v) ((e1 * (v[o] - v[o - SX]) + e2 * (v[o] - v[o + SX]) + e3 * (v[o] - v[o - SY]) + \
+                e4 * (v[o] - v[o + SY]) + e5 * (v[o] - v[o - 1]) + e6 * (v[o] - v[o + 1])) / cv_v)
+            c.s[S_FXV][o] = FV(vx);
+            c.s[S_FYV][o] = FV(vy);
+            c.s[S_FZV][o] = FV(vz);
+#undef FV
+        }
+        // CFL candidate of cell (i, j, k) (lagran.cpp:388-438)
+        const double gm = c.p.gamma;
+        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        double rho = c.f[SAMS_F_RHO][o];
+        double pressure = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ELECTRON][o] + (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ION][o];
+        double rho0 = pmax(rho, NONE_ZERO);
+        double cs2 = gm * pressure / rho0;
+        double w1 = (bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o]) / c.p.mu0 / rho0;
+        double c_visc2 = p_visc / rho0;
+        double length = pmin(pmin(dx, dy), dz);
+        double dt1 = length / (sqrt(c_visc2) + sqrt(cs2 + w1 + c_visc2));
+        double ax = 0.25 * (dy * dz), ay = 0.25 * (dx * dz), az = 0.25 * (dx * dy);
+        double vxbm = (vx[c_m00] + vx[c_mm0] + vx[c_m0m] + vx[c_mmm]) * ax;
+        double vxbp = (vx[c_000] + vx[c_0m0] + vx[c_00m] + vx[c_0mm]) * ax;
+        double vybm = (vy[c_0m0] + vy[c_mm0] + vy[c_0mm] + vy[c_mmm]) * ay;
+        double vybp = (vy[c_000] + vy[c_m00] + vy[c_00m] + vy[c_m0m]) * ay;
+        double vzbm = (vz[c_00m] + vz[c_m0m] + vz[c_0mm] + vz[c_mmm]) * az;
+        double vzbp = (vz[c_000] + vz[c_m00] + vz[c_0m0] + vz[c_mm0]) * az;
+        double dvx = fabs(vxbp - vxbm), dvy = fabs(vybp - vybm), dvz = fabs(vzbp - vzbm);
+        double avxm = fabs(vxbm), avxp = fabs(vxbp), avym = fabs(vybm);
+        double avyp = fabs(vybp), avzm = fabs(vzbm), avzp = fabs(vzbp);
+        double volume = cv;
+        double dt2 = volume / pmax(pmax(pmax(avxm, avxp), dvx), 1.0e-10 * volume);
+        double dt3 = volume / pmax(pmax(pmax(avym, avyp), dvy), 1.0e-10 * volume);
+        double dt4 = volume / pmax(pmax(pmax(avzm, avzp), dvz), 1.0e-10 * volume);
+        return pmin(pmin(pmin(dt1, dt2), dt3), dt4);
+    }
+};
+
+// Resistive sub-step, part 1: current density, eta (lagran.cpp:449-474,
+// evaluated at the same point from the same B, so computed once), edge
+// electric fields and Ohmic heating rate.
+struct ResistRK {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double dxc = c.ax.dxc[i + 2], dyc = c.ax.dyc[j + 2], dzc = c.ax.dzc[k + 2];
+        double jx1 = (bz[o + SY] - bz[o]) / dyc - (by[o + 1] - by[o]) / dzc;
+        double jx2 = (bz[o + SX + SY] - bz[o + SX]) / dyc - (by[o + SX + 1] - by[o + SX]) / dzc;
+        double jy1 = (bx[o + 1] - bx[o]) / dzc - (bz[o + SX] - bz[o]) / dxc;
+        double jy2 = (bx[o + SY + 1] - bx[o + SY]) / dzc - (bz[o + SX + SY] - bz[o + SY]) / dxc;
+        double jz1 = (by[o + SX] - by[o]) / dxc - (bx[o + SY] - bx[o]) / dyc;
+        double jz2 = (by[o + SX + 1] - by[o + 1]) / dxc - (bx[o + SY + 1] - bx[o + 1]) / dyc;
+        double jx = 0.5 * (jx1 + jx2), jy = 0.5 * (jy1 + jy2), jz = 0.5 * (jz1 + jz2);
+        double j_local = sqrt(jx * jx + jy * jy + jz * jz);
+        double eta = j_local > c.p.j_max ? c.p.eta_bg + c.p.eta0 : c.p.eta_bg;
+        c.s[S_FLUXX][o] = -jx * eta * dxc * 0.5;
+        c.s[S_FLUXY][o] = -jy * eta * dyc * 0.5;
+        c.s[S_FLUXZ][o] = -jz * eta * dzc * 0.5;
+        c.s[S_CURLB][o] = eta * (jx * jx + jy * jy + jz * jz);
+    }
+};
+
+// Resistive sub-step, part 2: constrained-transport B update and Ohmic
+// heating; on the last sub-step also keeps the pre-update face B as b1,
+// which the predictor reads (resistive_effects' copy, lagran.cpp:482-484).
+struct ResistB {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int last, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        const double *fx = c.s[S_FLUXX], *fy = c.s[S_FLUXY], *fz = c.s[S_FLUXZ];
+        const double dt = c.sc->dt_sub;
+        double bxo = bx[o], byo = by[o], bzo = bz[o];
+        if (last) {
+            c.s[S_B1X][o] = bxo;
+            c.s[S_B1Y][o] = byo;
+            c.s[S_B1Z][o] = bzo;
+        }
+        const bool inx = i >= 0 && i <= g.nx, iny = j >= 0 && j <= g.ny, inz = k >= 0 && k <= g.nz;
+        const bool inx1 = i >= 1 && i <= g.nx, iny1 = j >= 1 && j <= g.ny, inz1 = k >= 1 && k <= g.nz;
+        if (inx && iny1 && inz1) {
+            double area = c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
+            bx[o] = bxo + (fz[o] - fz[o - SY] + fz[o - 1] - fz[o - SY - 1] - fy[o] + fy[o - 1] - fy[o - SY] + fy[o - SY - 1]) * dt / area;
+        }
+        if (inx1 && iny && inz1) {
+            double area = c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
+            by[o] = byo + (fx[o] - fx[o - 1] + fx[o - SX] - fx[o - SX - 1] - fz[o] + fz[o - SX] - fz[o - 1] + fz[o - SX - 1]) * dt / area;
+        }
+        if (inx1 && iny1 && inz) {
+            double area = c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
+            bz[o] = bzo + (fy[o] - fy[o - SX] + fy[o - SY] - fy[o - SX - SY] - fx[o] + fx[o - SY] - fx[o - SX] + fx[o - SX - SY]) * dt / area;
+        }
+        if (inx1 && iny1 && inz1) {
+            const double *curlb = c.s[S_CURLB];
+            double sum_curlb = curlb[o] + curlb[o - SX] + curlb[o - SY] + curlb[o - SX - SY] +
+                               curlb[o - 1] + curlb[o - SX - 1] + curlb[o - SY - 1] + curlb[o - SX - SY - 1];
+            double *ee = c.f[SAMS_F_ENERGY_ELECTRON];
+            ee[o] += sum_curlb * dt / (8.0 * c.f[SAMS_F_RHO][o]);
+        }
+    }
+};
+
+// Predictor, part 1: half-step cell volume and B (then scaled by cv1), and
+// the half-step pressures (lagran.cpp:598-614, 806-882).
+struct Pred1 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+        const double dt = c.sc->dt;
+        const double dxb0 = c.ax.dxb[i + 2], dxbm = c.ax.dxb[i + 1];
+        const double dyb0 = c.ax.dyb[j + 2], dybm = c.ax.dyb[j + 1];
+        const double dzb0 = c.ax.dzb[k + 2], dzbm = c.ax.dzb[k + 1];
+        const double dxab0 = dyb0 * dzb0, dxabm = dyb0 * dzb0;          // dxab(i) and dxab(i-1)
+        const double dyab0 = dxb0 * dzb0, dyabm = dxb0 * dzb0;          // dyab(j) and dyab(j-1)
+        const double dzab0 = dxb0 * dyb0, dzabm = dxb0 * dyb0;          // dzab(k) and dzab(k-1)
+        (void)dxbm; (void)dybm; (void)dzbm;
+        const long long a = o, am = o - SX, bm = o - SY, cm = o - 1;
+        double vxb = 0.25 * (vx[a] + vx[bm] + vx[cm] + vx[bm - 1]);
+        double vxbm = 0.25 * (vx[am] + vx[am - SY] + vx[am - 1] + vx[am - SY - 1]);
+        double vyb = 0.25 * (vy[a] + vy[am] + vy[cm] + vy[am - 1]);
+        double vybm = 0.25 * (vy[bm] + vy[bm - SX] + vy[bm - 1] + vy[bm - SX - 1]);
+        double vzb = 0.25 * (vz[a] + vz[am] + vz[bm] + vz[am - SY]);
+        double vzbm = 0.25 * (vz[cm] + vz[am - 1] + vz[bm - 1] + vz[am - SY - 1]);
+        double vol = dxb0 * (dyb0 * dzb0);
+        double dvxdx = (vxb * dxab0 - vxbm * dxabm) / vol;
+        double dvydy = (vyb * dyab0 - vybm * dyabm) / vol;
+        double dvzdz = (vzb * dzab0 - vzbm * dzabm) / vol;
+        double dv = (dvxdx + dvydy + dvzdz) * dt / 2.0;
+        double cv1 = vol * (1.0 + dv);
+
+        vxb = 0.25 * (vx[a] + vx[am] + vx[cm] + vx[am - 1]);
+        vxbm = 0.25 * (vx[bm] + vx[bm - SX] + vx[bm - 1] + vx[bm - SX - 1]);
+        vyb = 0.25 * (vy[a] + vy[bm] + vy[cm] + vy[bm - 1]);
+        vybm = 0.25 * (vy[am] + vy[am - SY] + vy[am - 1] + vy[am - SY - 1]);
+        double dvxdy = (vxb * dyab0 - vxbm * dyabm) / vol;
+        double dvydx = (vyb * dxab0 - vybm * dxabm) / vol;
+
+        vxb = 0.25 * (vx[a] + vx[am] + vx[bm] + vx[am - SY]);
+        vxbm = 0.25 * (vx[cm] + vx[am - 1] + vx[bm - 1] + vx[am - SY - 1]);
+        double vzb2 = 0.25 * (vz[a] + vz[bm] + vz[cm] + vz[bm - 1]);
+        double vzbm2 = 0.25 * (vz[am] + vz[am - SY] + vz[am - 1] + vz[am - SY - 1]);
+        double dvxdz = (vxb * dzab0 - vxbm * dzabm) / vol;
+        double dvzdx = (vzb2 * dxab0 - vzbm2 * dxabm) / vol;
+
+        vyb = 0.25 * (vy[a] + vy[am] + vy[bm] + vy[am - SY]);
+        vybm = 0.25 * (vy[cm] + vy[am - 1] + vy[bm - 1] + vy[am - SY - 1]);
+        vzb2 = 0.25 * (vz[a] + vz[am] + vz[cm] + vz[am - 1]);
+        vzbm2 = 0.25 * (vz[bm] + vz[bm - SX] + vz[bm - 1] + vz[bm - SX - 1]);
+        double dvydz = (vyb * dzab0 - vybm * dzabm) / vol;
+        double dvzdy = (vzb2 * dyab0 - vzbm2 * dyabm) / vol;
+
+        double b1x, b1y, b1z;
+        if (resistive) {
+            b1x = c.s[S_B1X][o];
+            b1y = c.s[S_B1Y][o];
+            b1z = c.s[S_B1Z][o];
+        } else {
+            const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+            b1x = 0.5 * (bx[o] + bx[o - SX]);
+            b1y = 0.5 * (by[o] + by[o - SY]);
+            b1z = 0.5 * (bz[o] + bz[o - 1]);
+        }
+        double w3 = b1x * dvxdx + b1y * dvxdy + b1z * dvxdz;
+        double w4 = b1x * dvydx + b1y * dvydy + b1z * dvydz;
+        double w5 = b1x * dvzdx + b1y * dvzdy + b1z * dvzdz;
+        b1x = (b1x + w3 * dt / 2.0) / (1.0 + dv);
+        b1y = (b1y + w4 * dt / 2.0) / (1.0 + dv);
+        b1z = (b1z + w5 * dt / 2.0) / (1.0 + dv);
+        c.s[S_B1X][o] = b1x * cv1;
+        c.s[S_B1Y][o] = b1y * cv1;
+        c.s[S_B1Z][o] = b1z * cv1;
+        c.s[S_CV1][o] = cv1;
+
+        if (i < 0 || i > g.nx + 1 || j < 0 || j > g.ny + 1 || k < 0 || k > g.nz + 1) return;
+        const double gm = c.p.gamma;
+        double rho = c.f[SAMS_F_RHO][o], ee = c.f[SAMS_F_ENERGY_ELECTRON][o], ei = c.f[SAMS_F_ENERGY_ION][o];
+        double pe = resistive ? c.s[S_PE][o] : (gm - 1.0) * rho * ee;
+        double pi = (gm - 1.0) * rho * ei;
+        double dvv = cv1 / vol - 1.0;
+        double e1_e = ee - pe * dvv / rho;
+        double e1_i = ei - pi * dvv / rho;
+        e1_i += c.s[S_VH][o] * dt / 2.0 / rho;
+        c.s[S_PE][o] = e1_e * (gm - 1.0) * rho * vol / cv1;
+        c.s[S_PI][o] = e1_i * (gm - 1.0) * rho * vol / cv1;
+    }
+};
+
+// Predictor, part 2: pressure and J x B forces on nodes and the half-step
+// velocity (lagran.cpp:619-733, Cartesian).
+struct Pred2 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double *pe = c.s[S_PE], *pi = c.s[S_PI], *cv1 = c.s[S_CV1];
+        const double *bx1 = c.s[S_B1X], *by1 = c.s[S_B1Y], *bz1 = c.s[S_B1Z];
+        const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
+        const double dhy = dy, dhz = dz;
+        const long long q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
+                        qyz = o + SY + 1, qxyz = o + SX + SY + 1;
+        double pp = pe[q0] + pi[q0], ppx = pe[qx] + pi[qx], ppy = pe[qy] + pi[qy], ppz = pe[qz] + pi[qz];
+        double ppxy = pe[qxy] + pi[qxy], ppxz = pe[qxz] + pi[qxz], ppyz = pe[qyz] + pi[qyz], ppxyz = pe[qxyz] + pi[qxyz];
+        double w1 = pp + ppy + ppz + ppyz;
+        double w2 = ppx + ppxy + ppxz + ppxyz;
+        double fx = (w1 - w2) * 0.25 / dx;
+        w1 = pp + ppx + ppz + ppxz;
+        w2 = ppy + ppxy + ppyz + ppxyz;
+        double fy = (w1 - w2) * 0.25 / dhy;
+        w1 = pp + ppx + ppy + ppxy;
+        w2 = ppz + ppxz + ppyz + ppxyz;
+        double fz = (w1 - w2) * 0.25 / dhz;
+
+        double cvx = cv1[q0] + cv1[qy] + cv1[qz] + cv1[qyz];
+        double cvxp = cv1[qx] + cv1[qxy] + cv1[qxz] + cv1[qxyz];
+        double cvy = cv1[q0] + cv1[qx] + cv1[qz] + cv1[qxz];
+        double cvyp = cv1[qy] + cv1[qxy] + cv1[qyz] + cv1[qxyz];
+        double cvz = cv1[q0] + cv1[qx] + cv1[qy] + cv1[qxy];
+        double cvzp = cv1[qz] + cv1[qxz] + cv1[qyz] + cv1[qxyz];
+
+        w1 = (bz1[q0] + bz1[qx] + bz1[qz] + bz1[qxz]) / cvy;
+        w2 = (bz1[qy] + bz1[qxy] + bz1[qyz] + bz1[qxyz]) / cvyp;
+        double jx = (w2 - w1) / dhy;
+        w1 = (by1[q0] + by1[qx] + by1[qy] + by1[qxy]) / cvz;
+        w2 = (by1[qz] + by1[qxz] + by1[qyz] + by1[qxyz]) / cvzp;
+        jx -= (w2 - w1) / dhz;
+
+        w1 = (bz1[q0] + bz1[qy] + bz1[qz] + bz1[qyz]) / cvx;
+        w2 = (bz1[qx] + bz1[qxy] + bz1[qxz] + bz1[qxyz]) / cvxp;
+        double jy = -(w2 - w1) / dx;
+        w1 = (bx1[q0] + bx1[qx] + bx1[qy] + bx1[qxy]) / cvz;
+        w2 = (bx1[qz] + bx1[qxz] + bx1[qyz] + bx1[qxyz]) / cvzp;
+        jy += (w2 - w1) / dhz;
+
+        w1 = (by1[q0] + by1[qy] + by1[qz] + by1[qyz]) / cvx;
+        w2 = (by1[qx] + by1[qxy] + by1[qxz] + by1[qxyz]) / cvxp;
+        double jz = (w2 - w1) / dx;
+        w1 = (bx1[q0] + bx1[qx] + bx1[qz] + bx1[qxz]) / cvy;
+        w2 = (bx1[qy] + bx1[qxy] + bx1[qyz] + bx1[qxyz]) / cvyp;
+        jz -= (w2 - w1) / dhy;
+
+#define SUM8(a) (a[q0] + a[qx] + a[qy] + a[qxy] + a[qz] + a[qxz] + a[qyz] + a[qxyz])
+        double bxv = SUM8(bx1) / (cvx + cvxp);
+        double byv = SUM8(by1) / (cvx + cvxp);
+        double bzv = SUM8(bz1) / (cvx + cvxp);
+#undef SUM8
+        const double mu0 = c.p.mu0;
+        fx += (jy * bzv - jz * byv) / mu0;
+        fy += (jz * bxv - jx * bzv) / mu0;
+        fz += (jx * byv - jy * bxv) / mu0;
+        c.s[S_FX][o] = fx;
+        c.s[S_FY][o] = fy;
+        c.s[S_FZ][o] = fz;
+        const double dt = c.sc->dt;
+        const double rho_v = c.s[S_RHOV][o];
+        c.f[SAMS_F_VX1][o] = c.f[SAMS_F_VX][o] + dt / 2.0 * (c.s[S_FXV][o] + fx) / rho_v;
+        c.f[SAMS_F_VY1][o] = c.f[SAMS_F_VY][o] + dt / 2.0 * (c.s[S_FYV][o] + fy) / rho_v;
+        c.f[SAMS_F_VZ1][o] = c.f[SAMS_F_VZ][o] + dt / 2.0 * (c.s[S_FZV][o] + fz) / rho_v;
+    }
+};
+
+// Corrector, part 1: shock heating with the half-step velocities
+// (lagran.cpp:884-993, including its dy*dy factors at :987).
+struct Corr1 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+        const double *vx1 = c.f[SAMS_F_VX1], *vy1 = c.f[SAMS_F_VY1], *vz1 = c.f[SAMS_F_VZ1];
+        const double *a1a = c.s[S_A1], *a2a = c.s[S_A2], *a3a = c.s[S_A3];
+#define DD(a, b) (1 * ((vx[a] - vx[b]) * (vx1[a] - vx1[b]) + (vy[a] - vy[b]) * (vy1[a] - vy1[b]) + \
+                       (vz[a] - vz[b]) * (vz1[a] - vz1[b])))
+        const long long mm0 = o - SX - SY, m00 = o - SX, om0 = o - SY;
+        double a1 = DD(mm0, om0);
+        double a2 = DD(om0, o);
+        double a3 = DD(o, m00);
+        double a4 = DD(m00, mm0);
+        double a5 = DD(mm0 + 1, om0 + 1);
+        double a6 = DD(om0 + 1, o + 1);
+        double a7 = DD(o + 1, m00 + 1);
+        double a8 = DD(m00 + 1, mm0 + 1);
+        double a9 = DD(o - 1, o);
+        double a10 = DD(m00 - 1, m00);
+        double a11 = DD(mm0 - 1, mm0);
+        double a12 = DD(om0 - 1, om0);
+#undef DD
+        const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
+        double vh = (-0.25 * dy * dz * a1a[o] * a1 - 0.25 * dx * dz * a2a[o] * a2 - 0.25 * dy * dz * a1a[o + SY] * a3 -
+                     0.25 * dx * dz * a2a[o - SX] * a4 - 0.25 * dy * dz * a1a[o + 1] * a5 - 0.25 * dx * dz * a2a[o + 1] * a6 -
+                     0.25 * dy * dz * a1a[o + SY + 1] * a7 - 0.25 * dx * dz * a2a[o - SX + 1] * a8 - 0.25 * dy * dy * a3a[o] * a9 -
+                     0.25 * dx * dy * a3a[o - SX] * a10 - 0.25 * dy * dy * a3a[o - SX - SY] * a11 - 0.25 * dx * dy * a3a[o - SY] * a12);
+        c.s[S_VH][o] = pmax(vh / (dx * (dy * dz)), 0.0);
+    }
+};
+
+// Corrector, part 2: final velocities on nodes; energies, density on cells
+// (lagran.cpp:754-798).  The corrector's cv1 is not kept: the x sweep
+// recomputes it over the whole range before any read.
+struct Corr2 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double dt = c.sc->dt;
+        {
+            const double rho_v = c.s[S_RHOV][o];
+            double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+            vx[o] += dt * (c.s[S_FXV][o] + c.s[S_FX][o]) / rho_v;
+            vy[o] += dt * (c.s[S_FYV][o] + c.s[S_FY][o]) / rho_v;
+            vz[o] += dt * (c.s[S_FZV][o] + c.s[S_FZ][o]) / rho_v;
+        }
+        if (i < 1 || j < 1 || k < 1) return;
+        const double *vx1 = c.f[SAMS_F_VX1], *vy1 = c.f[SAMS_F_VY1], *vz1 = c.f[SAMS_F_VZ1];
+        const long long a = o, am = o - SX, bm = o - SY, cm = o - 1;
+        double vxb = 0.25 * (vx1[a] + vx1[bm] + vx1[cm] + vx1[bm - 1]);
+        double vxbm = 0.25 * (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]);
+        double vyb = 0.25 * (vy1[a] + vy1[am] + vy1[cm] + vy1[am - 1]);
+        double vybm = 0.25 * (vy1[bm] + vy1[bm - SX] + vy1[bm - 1] + vy1[bm - SX - 1]);
+        double vzb = 0.25 * (vz1[a] + vz1[am] + vz1[bm] + vz1[am - SY]);
+        double vzbm = 0.25 * (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]);
+        const double dxb0 = c.ax.dxb[i + 2], dyb0 = c.ax.dyb[j + 2], dzb0 = c.ax.dzb[k + 2];
+        double vol = dxb0 * (dyb0 * dzb0);
+        double dvxdx = (vxb * (dyb0 * dzb0) - vxbm * (dyb0 * dzb0)) / vol;
+        double dvydy = (vyb * (dxb0 * dzb0) - vybm * (dxb0 * dzb0)) / vol;
+        double dvzdz = (vzb * (dxb0 * dyb0) - vzbm * (dxb0 * dyb0)) / vol;
+        double dv = (dvxdx + dvydy + dvzdz) * dt;
+        double *rho = c.f[SAMS_F_RHO], *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+        double r = rho[o];
+        ee[o] -= dv * c.s[S_PE][o] / r;
+        ei[o] += (dt * c.s[S_VH][o] - dv * c.s[S_PI][o]) / r;
+        rho[o] = r / (1.0 + dv);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Remap
+// ---------------------------------------------------------------------------
+
+// B to flux form (remap.cpp:46-50) when arg = 0, back to B with the
+// none_zero guard (remap.cpp:91-95) when arg = 1.
+struct BScale {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int back, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long o = LOFF(i, j, k);
+        if (j >= -1 && k >= -1) {
+            double a = dxab_at(c, i, j, k);
+            double *b = c.f[SAMS_F_BX];
+            b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
+        }
+        if (i >= -1 && k >= -1) {
+            double a = dyab_at(c, i, j, k);
+            double *b = c.f[SAMS_F_BY];
+            b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
+        }
+        if (i >= -1 && j >= -1) {
+            double a = dzab_at(c, i, j, k);
+            double *b = c.f[SAMS_F_BZ];
+            b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
+        }
+    }
+};
+
+__device__ __forceinline__ long long dir_stride(const Geom &g, int dir)
+{
+    return dir == 0 ? g.sx : (dir == 1 ? g.sy : 1);
+}
+
+// First pass of a sweep: volumes before/after the sweep and the sweep-axis
+// cell length before it (xremap.cpp:28-70, yremap.cpp:27-80,
+// zremap.cpp:28-81); also rho1 = rho and dm = 0 (xremap.cpp:24-25).
+// Terms multiplied by a zero pass flag are left out: 0 * finite = 0 and
+// adding zero does not change the sum.
+template <int DIR>
+struct SweepVol {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double dt = c.sc->dt;
+        const double dxb0 = c.ax.dxb[i + 2], dyb0 = c.ax.dyb[j + 2], dzb0 = c.ax.dzb[k + 2];
+        const double vol = dxb0 * (dyb0 * dzb0);
+        const long long am = o - SX, bm = o - SY, cm = o - 1;
+        double tx = 0.0, ty = 0.0, tz = 0.0, vxb = 0.0, vxbm = 0.0, vyb = 0.0, vybm = 0.0, vzb = 0.0, vzbm = 0.0;
+        if (DIR == 0) {
+            const double *vx1 = c.f[SAMS_F_VX1];
+            vxb = (vx1[o] + vx1[bm] + vx1[cm] + vx1[bm - 1]) * 0.25;
+            vxbm = (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]) * 0.25;
+            tx = vxb * (dyb0 * dzb0) - vxbm * (dyb0 * dzb0);
+        }
+        if (DIR <= 1) {
+            const double *vy1 = c.f[SAMS_F_VY1];
+            vyb = (vy1[o] + vy1[am] + vy1[cm] + vy1[am - 1]) * 0.25;
+            vybm = (vy1[bm] + vy1[bm - SX] + vy1[bm - 1] + vy1[bm - SX - 1]) * 0.25;
+            ty = vyb * (dxb0 * dzb0) - vybm * (dxb0 * dzb0);
+        }
+        {
+            const double *vz1 = c.f[SAMS_F_VZ1];
+            vzb = (vz1[o] + vz1[am] + vz1[bm] + vz1[am - SY]) * 0.25;
+            vzbm = (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]) * 0.25;
+            tz = vzb * (dxb0 * dyb0) - vzbm * (dxb0 * dyb0);
+        }
+        double dv, cv2, db1;
+        if (DIR == 0) {
+            double dvxdx = tx / vol, dvydy = 1.0 * ty / vol, dvzdz = 1.0 * tz / vol;
+            dv = (dvydy + dvzdz) * dt;
+            cv2 = vol * (1.0 + dv);
+            dv = dv + dvxdx * dt;
+            db1 = dxb0 + (vxb - vxbm) * dt;
+        } else if (DIR == 1) {
+            double dvydy = ty / vol, dvzdz = 1.0 * tz / vol;
+            dv = dvzdz * dt;
+            cv2 = vol * (1.0 + dv);
+            dv = dv + dvydy * dt;
+            db1 = dyb0 + (vyb - vybm) * dt;
+        } else {
+            double dvzdz = tz / vol;
+            dv = 0.0 * dt;
+            cv2 = vol * (1.0 + dv);
+            dv = dv + dvzdz * dt;
+            db1 = dzb0 + (vzb - vzbm) * dt;
+        }
+        c.s[S_R_CV2][o] = cv2;
+        c.s[S_R_CV1][o] = vol * (1.0 + dv);
+        c.s[S_R_DB1][o] = db1;
+        c.s[S_R_RHO1][o] = c.f[SAMS_F_RHO][o];
+        c.f[SAMS_F_DM][o] = 0.0;
+    }
+};
+
+struct SweepCvc {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double *cv1 = c.s[S_R_CV1];
+        c.s[S_R_CVC1][o] = 0.125 * (cv1[o] + cv1[o + SX] + cv1[o + SY] + cv1[o + SX + SY] +
+                                    cv1[o + 1] + cv1[o + SX + 1] + cv1[o + SY + 1] + cv1[o + SX + SY + 1]);
+    }
+};
+
+// Both constrained-transport fluxes of a sweep.
+template <int DIR>
+struct SweepCT {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const long long d = dir_stride(g, DIR);
+        const double dt = c.sc->dt;
+        const double *db1 = c.s[S_R_DB1], *cvc1 = c.s[S_R_CVC1], *cv1 = c.s[S_R_CV1];
+        const double *v1 = c.f[SAMS_F_VX1 + DIR];
+        // transverse offsets of the two db1 samples averaged for each flux
+        long long t1, t2, va1, va2;
+        const double *b1, *b2;
+        if (DIR == 0) {        // vx_by (avg +y, v avg -z), vx_bz (avg +z, v avg -y)
+            t1 = SY; va1 = -1; b1 = c.f[SAMS_F_BY];
+            t2 = 1;  va2 = -SY; b2 = c.f[SAMS_F_BZ];
+        } else if (DIR == 1) { // vy_bx (avg +x, v avg -z), vy_bz (avg +z, v avg -x)
+            t1 = SX; va1 = -1; b1 = c.f[SAMS_F_BX];
+            t2 = 1;  va2 = -SX; b2 = c.f[SAMS_F_BZ];
+        } else {               // vz_bx (avg +x, v avg -y), vz_by (avg +y, v avg -x)
+            t1 = SX; va1 = -SY; b1 = c.f[SAMS_F_BX];
+            t2 = SY; va2 = -SX; b2 = c.f[SAMS_F_BY];
+        }
+        const double dci = cvc1[o], dcm = cvc1[o - d], dcp = cvc1[o + d], cvi = cv1[o], cvp = cv1[o + d];
+        {
+            double v = (v1[o] + v1[o + va1]) * 0.5;
+            double dbm = (db1[o - d] + db1[o - d + t1]) * 0.5, dbi = (db1[o] + db1[o + t1]) * 0.5;
+            double dbp = (db1[o + d] + db1[o + d + t1]) * 0.5, dbp2 = (db1[o + 2 * d] + db1[o + 2 * d + t1]) * 0.5;
+            c.s[S_R_CT1][o] = ct_flux(v, dt, b1[o - d], b1[o], b1[o + d], b1[o + 2 * d], dbm, dbi, dbp, dbp2,
+                                      dci, dcm, dcp, cvi, cvp);
+        }
+        {
+            double v = (v1[o] + v1[o + va2]) * 0.5;
+            double dbm = (db1[o - d] + db1[o - d + t2]) * 0.5, dbi = (db1[o] + db1[o + t2]) * 0.5;
+            double dbp = (db1[o + d] + db1[o + d + t2]) * 0.5, dbp2 = (db1[o + 2 * d] + db1[o + 2 * d + t2]) * 0.5;
+            c.s[S_R_CT2][o] = ct_flux(v, dt, b2[o - d], b2[o], b2[o + d], b2[o + 2 * d], dbm, dbi, dbp, dbp2,
+                                      dci, dcm, dcp, cvi, cvp);
+        }
+        (void)SX;
+    }
+};
+
+// Both constrained-transport updates of a sweep (xremap.cpp:87-115,
+// yremap.cpp:97-127, zremap.cpp:103-121), in the reference's order.
+template <int DIR>
+struct SweepCTUpd {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double *f1 = c.s[S_R_CT1], *f2 = c.s[S_R_CT2];
+        double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        const bool xb = i >= 0, xc = i >= 1, yb = j >= 0, yc = j >= 1, zb = k >= 0, zc = k >= 1;
+        if (DIR == 0) {
+            if (xc && yb && zc) by[o] = by[o] - f1[o] + f1[o - SX];
+            if (xc && yc && zb) bz[o] = bz[o] - f2[o] + f2[o - SX];
+            if (xb && yc && zc) {
+                double t = bx[o] + f1[o] - f1[o - SY];
+                bx[o] = t + f2[o] - f2[o - 1];
+            }
+        } else if (DIR == 1) {
+            if (xb && yc && zc) bx[o] = bx[o] - f1[o] + f1[o - SY];
+            if (xc && yc && zb) bz[o] = bz[o] - f2[o] + f2[o - SY];
+            if (xc && yb && zc) {
+                double t = by[o] + f1[o] - f1[o - SX];
+                by[o] = t + f2[o] - f2[o - 1];
+            }
+        } else {
+            if (xb && yc && zc) bx[o] = bx[o] - f1[o] + f1[o - 1];
+            if (xc && yb && zc) by[o] = by[o] - f2[o] + f2[o - 1];
+            if (xc && yc && zb) {
+                double t = bz[o] + f1[o] - f1[o - SX];
+                bz[o] = t + f2[o] - f2[o - SY];
+            }
+        }
+    }
+};
+
+// Node-average advection velocity of a cell face along the sweep
+// (x/y/z_mass_flux and x/y/z_energy_flux use the same 4-point sums).
+template <int DIR>
+__device__ __forceinline__ double face_velocity(const Ctx &c, long long o)
+{
+    const Geom &g = c.g;
+    const long long SX = g.sx, SY = g.sy;
+    if (DIR == 0) {
+        const double *v = c.f[SAMS_F_VX1];
+        return (v[o] + v[o - SY] + v[o - 1] + v[o - SY - 1]) * 0.25;
+    } else if (DIR == 1) {
+        const double *v = c.f[SAMS_F_VY1];
+        return (v[o - SX] + v[o] + v[o - SX - 1] + v[o - 1]) * 0.25;
+    } else {
+        const double *v = c.f[SAMS_F_VZ1];
+        return (v[o - SX] + v[o] + v[o - SX - SY] + v[o - SY]) * 0.25;
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ double face_area(const Ctx &c, int i, int j, int k)
+{
+    return DIR == 0 ? dxab_at(c, i, j, k) : (DIR == 1 ? dyab_at(c, i, j, k) : dzab_at(c, i, j, k));
+}
+
+template <int DIR>
+struct SweepMass {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, DIR == 0 ? g.nx : g.nx + 1, 0, DIR == 1 ? g.ny : g.ny + 1, 0,
+                   DIR == 2 ? g.nz : g.nz + 1);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long o = LOFF(i, j, k);
+        const long long d = dir_stride(g, DIR);
+        const double *rho = c.f[SAMS_F_RHO], *cvc1 = c.s[S_R_CVC1], *cv1 = c.s[S_R_CV1];
+        double v = face_velocity<DIR>(c, o);
+        c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
+                                      rho[o + 2 * d], cvc1[o], cvc1[o - d], cvc1[o + d], cv1[o], cv1[o + d]);
+    }
+};
+
+// Range lo/hi of index q in dimension DIM for a sweep-direction-dependent
+// interval: [alo, ahi] along the sweep, [blo, bhi] across it.
+template <int DIR, int DIM>
+__device__ __forceinline__ bool in_sweep_range(int q, int n, int alo, int ahi_off, int blo, int bhi_off)
+{
+    return DIM == DIR ? (q >= alo && q <= n + ahi_off) : (q >= blo && q <= n + bhi_off);
+}
+
+// rho update, energy fluxes, vertex density, node cv2, node dm and the v1
+// shift (xremap.cpp:121-221 and the y/z analogues).
+template <int DIR>
+struct SweepS6 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, DIR == 0 ? -2 : 0, DIR == 0 ? g.nx + 1 : g.nx, DIR == 1 ? -2 : 0,
+                   DIR == 1 ? g.ny + 1 : g.ny, DIR == 2 ? -2 : 0, DIR == 2 ? g.nz + 1 : g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const long long d = dir_stride(g, DIR);
+        const double dt = c.sc->dt;
+        const double *rho1 = c.s[S_R_RHO1], *cv1 = c.s[S_R_CV1], *cv2 = c.s[S_R_CV2], *cvc1 = c.s[S_R_CVC1];
+        const double *dm = c.f[SAMS_F_DM];
+        const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+        const int qd = DIR == 0 ? i : (DIR == 1 ? j : k);
+        const bool all0n = i >= 0 && i <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
+        // density (1..n)^3
+        if (i >= 1 && j >= 1 && k >= 1 && i <= g.nx && j <= g.ny && k <= g.nz)
+            c.f[SAMS_F_RHO][o] = (rho1[o] * cv1[o] + dm[o - d] - dm[o]) / cv2[o];
+        // energy fluxes (0..n)^3
+        if (all0n) {
+            double v = face_velocity<DIR>(c, o);
+            double area = face_area<DIR>(c, i, j, k);
+            const double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+            c.s[S_R_FE1][o] = energy_flux(v, dt, area, ee[o - d], ee[o], ee[o + d], ee[o + 2 * d], cvc1[o], cvc1[o - d],
+                                          cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]);
+            c.s[S_R_FE2][o] = energy_flux(v, dt, area, ei[o - d], ei[o], ei[o + d], ei[o + 2 * d], cvc1[o], cvc1[o - d],
+                                          cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]);
+            // node cv2 (0..n)^3
+            c.s[S_R_CV2N][o] = (cv2[o] + cv2[o + SX] + cv2[o + SY] + cv2[o + SX + SY] +
+                                cv2[o + 1] + cv2[o + SX + 1] + cv2[o + SY + 1] + cv2[o + SX + SY + 1]) * 0.125;
+        }
+        // vertex density: -1..n+1 along the sweep, 0..n across
+        if (qd >= -1) {
+            double sum = rho1[o] * cv1[o] + rho1[o + SX] * cv1[o + SX] + rho1[o + SY] * cv1[o + SY] +
+                         rho1[o + SX + SY] * cv1[o + SX + SY] + rho1[o + 1] * cv1[o + 1] +
+                         rho1[o + SX + 1] * cv1[o + SX + 1] + rho1[o + SY + 1] * cv1[o + SY + 1] +
+                         rho1[o + SX + SY + 1] * cv1[o + SX + SY + 1];
+            c.s[S_R_RVN][o] = DIR == 0 ? sum * 0.125 / cvc1[o] : sum * (0.125 / cvc1[o]);
+        }
+        // node dm: -1..n along the sweep, 0..n across
+        if (qd >= -1 && qd <= nd) {
+            c.s[S_R_DMN][o] = (dm[o] + dm[o + SX] + dm[o + SY] + dm[o + SX + SY] +
+                               dm[o + 1] + dm[o + SX + 1] + dm[o + SY + 1] + dm[o + SX + SY + 1]) * 0.125;
+        }
+        // sweep-direction v1 moved to the face centre: -2..n+1 along, 0..n across
+        {
+            const double *v1 = c.f[SAMS_F_VX1 + DIR];
+            c.s[S_R_V1S][o] = (v1[o] + v1[o + d]) * 0.5;
+        }
+    }
+};
+
+// Energy updates (1..n)^3 and the three momentum fluxes (times dm).
+template <int DIR>
+struct SweepS7 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, DIR == 0 ? -1 : 0, g.nx, DIR == 1 ? -1 : 0, g.ny, DIR == 2 ? -1 : 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long o = LOFF(i, j, k);
+        const long long d = dir_stride(g, DIR);
+        const double dt = c.sc->dt;
+        const double *rho1 = c.s[S_R_RHO1], *cv1 = c.s[S_R_CV1], *cv2 = c.s[S_R_CV2], *cvc1 = c.s[S_R_CVC1];
+        if (i >= 1 && j >= 1 && k >= 1) {
+            const double *f1 = c.s[S_R_FE1], *f2 = c.s[S_R_FE2];
+            double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+            double den = cv2[o] * c.f[SAMS_F_RHO][o];
+            ee[o] = (ee[o] * cv1[o] * rho1[o] + f1[o - d] - f1[o]) / den;
+            ei[o] = (ei[o] * cv1[o] * rho1[o] + f2[o - d] - f2[o]) / den;
+        }
+        const double *v1s = c.s[S_R_V1S], *rv = c.s[S_R_RVN], *dmn = c.s[S_R_DMN];
+        // x sweep uses dxac; the y and z sweeps both use dyac (zremap.cpp:475)
+        double area = DIR == 0 ? dxac_at(c, i, j, k) : dyac_at(c, i, j, k);
+        const double v = v1s[o], dmv = dmn[o];
+        const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
+        const double rvi = rv[o], rvp = rv[o + d];
+        const double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
+        c.s[S_R_FM1][o] = mom_flux_dm<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
+                                                cvi, cvp, rvi, rvp, dmv);
+        c.s[S_R_FM2][o] = mom_flux_dm<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
+                                                cvi, cvp, rvi, rvp, dmv);
+        c.s[S_R_FM3][o] = mom_flux_dm<DIR == 2>(v, dt, area, uz[o - d], uz[o], uz[o + d], uz[o + 2 * d], dci, dcm, dcp,
+                                                cvi, cvp, rvi, rvp, dmv);
+    }
+};
+
+// Momentum updates with the vertex density after the sweep formed inline
+// (xremap.cpp:226-261).
+template <int DIR>
+struct SweepS8 {
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        const long long o = LOFF(i, j, k);
+        const long long d = dir_stride(g, DIR);
+        const double *rv = c.s[S_R_RVN], *cvc1 = c.s[S_R_CVC1], *cv2n = c.s[S_R_CV2N], *dmn = c.s[S_R_DMN];
+        const double rvo = rv[o], cvco = cvc1[o], cv2o = cv2n[o];
+        const double rho_v1 = (rvo * cvco + dmn[o - d] - dmn[o]) / cv2o;
+        const double den = cv2o * rho_v1;
+        double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
+        const double *f1 = c.s[S_R_FM1], *f2 = c.s[S_R_FM2], *f3 = c.s[S_R_FM3];
+        ux[o] = (rvo * ux[o] * cvco + f1[o - d] - f1[o]) / den;
+        uy[o] = (rvo * uy[o] * cvco + f2[o - d] - f2[o]) / den;
+        uz[o] = (rvo * uz[o] * cvco + f3[o - d] - f3[o]) / den;
+    }
+};
+
+#undef LOFF
+
+}  // namespace ops
+}  // namespace sams

@@ -1,0 +1,579 @@
+// lare_solver.cu -- kernels and step orchestration of one LARE3D solve.
+//
+// One step on the device, in launch order (reference events in brackets):
+//   [startOfTimestep -> lagrangian_step, lagran.cpp:95-173]
+//     CellPrep, NodePrep, Alpha, Visc (+ CFL block minima), DtFinalize,
+//     resistive only: 2 x {ResistRK, ResistB, fill B + energies},
+//     Pred1, Pred2, fill v1
+//   [halfTimestep -> corrector_step, lagran.cpp:739-804]
+//     Corr1, Corr2, fill v + energies + density
+//   [endOfTimestep -> eulerian_remap, remap.cpp:23-111]
+//     BScale, 3 x {SweepVol, SweepCvc, SweepCT, SweepCTUpd, SweepMass,
+//                  fill dm along the sweep, SweepS6, SweepS7, SweepS8,
+//                  fill the nine state fields}, BUnscale, fill B
+// The runner's step++/time += dt (runner.h:573-574) happens in DtFinalize.
+// Nothing is read back to the host inside a step.
+#include "lare_solver.cuh"
+#include "lare_ops.cuh"
+
+#include <cstdio>
+#include <cstring>
+
+namespace sams {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// One thread per (j, k) of a plane, blockIdx.y walks i.
+template <class Op>
+__global__ void __launch_bounds__(kThreads) k_op(Ctx c, int arg)
+{
+    int lo[3], hi[3];
+    Op::bounds(c.g, arg, lo, hi);
+    const int nk = hi[2] - lo[2] + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long plane = (long long)(hi[1] - lo[1] + 1) * nk;
+    if (t >= plane) return;
+    const int j = lo[1] + (int)(t / nk);
+    const int k = lo[2] + (int)(t % nk);
+    for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::run(c, arg, i, j, k);
+}
+
+// Visc with the CFL minimum: each block reduces its candidates and folds
+// them into Scalars::dtmin_bits.  Positive doubles order like their bit
+// patterns, so an integer atomicMin is an exact, order-free minimum.
+__global__ void __launch_bounds__(kThreads) k_visc(Ctx c)
+{
+    int lo[3], hi[3];
+    ops::Visc::bounds(c.g, 0, lo, hi);
+    const int nk = hi[2] - lo[2] + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long plane = (long long)(hi[1] - lo[1] + 1) * nk;
+    double best = DBL_MAX;
+    if (t < plane) {
+        const int j = lo[1] + (int)(t / nk);
+        const int k = lo[2] + (int)(t % nk);
+        for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) {
+            double cand = ops::Visc::run(c, 0, i, j, k);
+            best = dev::pmin(best, cand);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) best = dev::pmin(best, __shfl_xor_sync(0xffffffffu, best, off));
+    __shared__ double wmin[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = wmin[0];
+        for (int w = 1; w < kThreads / 32; ++w) m = dev::pmin(m, wmin[w]);
+        if (m < DBL_MAX) atomicMin(&c.sc->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// dt = dt_multiplier * min (lagran.cpp:387-442), then the runner's
+// min-with-DBL_MAX (runner.h:161-167, shared_data.h:428-440); the resistive
+// sub-step is dt / (int(dt/dtr) + 1) (lagran.cpp:159-163); dtr == dt, so
+// that count is 2.  Also the runner's time += dt, step++.
+__global__ void k_dt_finalize(Scalars *sc, double dt_multiplier, int resistive)
+{
+    double m = __longlong_as_double((long long)sc->dtmin_bits);
+    double dt = dt_multiplier * m;
+    sc->dtr = dt;
+    dt = dt < DBL_MAX ? dt : DBL_MAX;
+    sc->dt = dt;
+    if (resistive) {
+        int nsub = (int)(dt / sc->dtr) + 1;
+        sc->nsub = nsub;
+        sc->dt_sub = dt / (double)nsub;
+    }
+    sc->dtmin_bits = (unsigned long long)__double_as_longlong(DBL_MAX);
+    if (!(dt > 0.0) || !(dt < DBL_MAX)) sc->status = 1;
+    sc->time += dt;
+    sc->step += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Boundary fills (variableDef::applyBoundaryConditions order,
+// include/harness/variableDef.h:539-605; built-in conditions of
+// include/boundaryConditions/builtInBoundaryConditions.h).
+// ---------------------------------------------------------------------------
+
+struct FieldList {
+    int n;
+    int id[SAMS_NFIELDS];
+};
+
+__device__ __forceinline__ int field_lb(int f, int d) { return field_half(f, d) ? -2 : -1; }
+
+// All-periodic fields: applying the lower then upper periodic copy in x, y
+// and z in turn leaves every ghost point equal to the interior point it
+// wraps to, w(q) = q + n for q <= 0 and q - n for q >= n + 1 (a half-cell
+// index n keeps its value), so all ghosts are filled by one gather.
+__global__ void __launch_bounds__(kThreads) k_bc_periodic(Ctx c, FieldList fl)
+{
+    const int f = fl.id[blockIdx.y];
+    const Geom &g = c.g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    int lb[3], ext[3], gh[3];
+    for (int d = 0; d < 3; ++d) {
+        lb[d] = field_lb(f, d);
+        ext[d] = n[d] + 3 - lb[d];
+        gh[d] = ext[d] - n[d];
+    }
+    const long long A = (long long)gh[0] * ext[1] * ext[2];
+    const long long B = (long long)n[0] * gh[1] * ext[2];
+    const long long C = (long long)n[0] * n[1] * gh[2];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int q[3];
+    if (t < A) {
+        int gi = (int)(t / ((long long)ext[1] * ext[2]));
+        long long r = t % ((long long)ext[1] * ext[2]);
+        q[0] = gi < 1 - lb[0] ? lb[0] + gi : n[0] + 1 + (gi - (1 - lb[0]));
+        q[1] = lb[1] + (int)(r / ext[2]);
+        q[2] = lb[2] + (int)(r % ext[2]);
+    } else if ((t -= A) < B) {
+        int i = (int)(t / ((long long)gh[1] * ext[2]));
+        long long r = t % ((long long)gh[1] * ext[2]);
+        int gj = (int)(r / ext[2]);
+        q[0] = 1 + i;
+        q[1] = gj < 1 - lb[1] ? lb[1] + gj : n[1] + 1 + (gj - (1 - lb[1]));
+        q[2] = lb[2] + (int)(r % ext[2]);
+    } else if ((t -= B) < C) {
+        int i = (int)(t / ((long long)n[1] * gh[2]));
+        long long r = t % ((long long)n[1] * gh[2]);
+        int gk = (int)(r % gh[2]);
+        q[0] = 1 + i;
+        q[1] = 1 + (int)(r / gh[2]);
+        q[2] = gk < 1 - lb[2] ? lb[2] + gk : n[2] + 1 + (gk - (1 - lb[2]));
+    } else {
+        return;
+    }
+    int s[3];
+    for (int d = 0; d < 3; ++d) s[d] = q[d] <= 0 ? q[d] + n[d] : (q[d] >= n[d] + 1 ? q[d] - n[d] : q[d]);
+    double *a = c.f[f];
+    a[box_off(g, q[0], q[1], q[2])] = a[box_off(g, s[0], s[1], s[2])];
+}
+
+// One (dimension, edge) of the given fields, exactly as the reference's
+// boundary-condition objects apply it.
+__global__ void __launch_bounds__(kThreads) k_bc_edge(Ctx c, FieldList fl, BcTable bt, int d, int e)
+{
+    const int f = fl.id[blockIdx.y];
+    const int kind = bt.kind[f][d][e];
+    if (kind == SAMS_BC_NONE) return;
+    const Geom &g = c.g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    int lo[3], hi[3];
+    for (int q = 0; q < 3; ++q) {
+        lo[q] = field_lb(f, q);
+        hi[q] = n[q] + 2;
+    }
+    const bool half = field_half(f, d) != 0;
+    const int dlb = half ? 0 : 1, dub = n[d];
+    const int glo = e == 0 ? lo[d] : (half ? n[d] : n[d] + 1);
+    const int ghi = e == 0 ? 0 : n[d] + 2;
+    const int cnt = ghi - glo + 1;
+    lo[d] = glo;
+    hi[d] = ghi;
+    const int e1 = hi[1] - lo[1] + 1, e2 = hi[2] - lo[2] + 1;
+    const long long total = (long long)(hi[0] - lo[0] + 1) * e1 * e2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int q[3];
+    q[0] = lo[0] + (int)(t / ((long long)e1 * e2));
+    q[1] = lo[1] + (int)((t / e2) % e1);
+    q[2] = lo[2] + (int)(t % e2);
+    const int gq = q[d];
+    int s[3] = {q[0], q[1], q[2]};
+    double *a = c.f[f];
+    double v;
+    switch (kind) {
+    case SAMS_BC_PERIODIC:
+        s[d] = e == 0 ? dub - cnt + 1 + (gq - glo) : dlb + (gq - glo);
+        v = a[box_off(g, s[0], s[1], s[2])];
+        break;
+    case SAMS_BC_ZERO_GRADIENT:
+        s[d] = e == 0 ? dlb : dub;
+        v = a[box_off(g, s[0], s[1], s[2])];
+        break;
+    case SAMS_BC_MIRROR: {
+        const int last = e == 0 ? dlb : dub;
+        const int first = e == 0 ? ghi : glo;
+        int lt[3] = {q[0], q[1], q[2]};
+        lt[d] = last;
+        double av = a[box_off(g, lt[0], lt[1], lt[2])];
+        double bv = (av + av) / 2.0;
+        s[d] = last - (gq - first);
+        double delta = a[box_off(g, s[0], s[1], s[2])] - bv;
+        v = bv - delta;
+        break;
+    }
+    case SAMS_BC_CLAMP:
+        v = bt.value[f][d][e];
+        break;
+    default:
+        return;
+    }
+    a[box_off(g, q[0], q[1], q[2])] = v;
+}
+
+FieldList make_list(unsigned mask)
+{
+    FieldList fl{};
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        if (mask & (1u << f)) fl.id[fl.n++] = f;
+    return fl;
+}
+
+long long ceil_div(long long a, long long b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+Solver::~Solver() { free_all(); }
+
+void Solver::free_all()
+{
+    if (device_ >= 0) cudaSetDevice(device_);
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    if (arena_) cudaFree(arena_);
+    if (axes_) cudaFree(axes_);
+    if (sc_) cudaFree(sc_);
+    if (own_stream_) cudaStreamDestroy(own_stream_);
+    arena_ = nullptr;
+    axes_ = nullptr;
+    sc_ = nullptr;
+    own_stream_ = nullptr;
+}
+
+int Solver::check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return SAMS_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? SAMS_ERR_NOMEM : SAMS_ERR_CUDA;
+}
+
+static void axis_host(double lo, double hi, long long n, std::vector<double> &db, std::vector<double> &dc)
+{
+    // axisRegistry: b(i) = lo + d*i, c(i) = 0.5*(b(i) + b(i-1)), deltas with
+    // the first one copied from the next (non-periodic axes).
+    std::vector<double> b(n + 5), c(n + 5);
+    double d = (hi - lo) / (double)n;
+    for (long long i = -2; i <= n + 2; ++i) b[i + 2] = lo + d * (double)i;
+    for (long long i = -1; i <= n + 2; ++i) c[i + 2] = 0.5 * (b[i + 2] + b[i + 1]);
+    db.assign(n + 6, 0.0);
+    dc.assign(n + 6, 0.0);
+    for (long long i = -1; i <= n + 2; ++i) db[i + 2] = b[i + 2] - b[i + 1];
+    db[0] = db[1];
+    for (long long i = 0; i <= n + 2; ++i) dc[i + 2] = c[i + 2] - c[i + 1];
+    dc[1] = dc[2];
+}
+
+int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device)
+{
+    if (p.nx < 1 || p.ny < 1 || p.nz < 1) { err = "grid sizes must be >= 1"; return SAMS_ERR_INVALID; }
+    if (p.nx > 60000 || p.ny > 60000 || p.nz > 60000) { err = "grid size too large"; return SAMS_ERR_INVALID; }
+    if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
+    if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) {
+        err = "empty domain";
+        return SAMS_ERR_INVALID;
+    }
+    p_ = p;
+    device_ = device;
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 2; ++e) {
+                int k = bcs.kind[f][d][e];
+                if (k < SAMS_BC_NONE || k > SAMS_BC_CLAMP) { err = "unknown boundary-condition kind"; return SAMS_ERR_INVALID; }
+                bc_.kind[f][d][e] = (signed char)k;
+                bc_.value[f][d][e] = bcs.value[f][d][e];
+            }
+    int rc;
+    if ((rc = check(cudaSetDevice(device), "cudaSetDevice"))) return rc;
+    if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    stream_ = own_stream_;
+
+    Geom &g = ctx_.g;
+    g.nx = (int)p.nx;
+    g.ny = (int)p.ny;
+    g.nz = (int)p.nz;
+    g.zoff = 3;
+    const long long zrow = ((p.nz + 6) + 7) / 8 * 8;
+    g.sy = zrow;
+    g.sx = (long long)(p.ny + 5) * zrow;
+    g.nelem = (long long)(p.nx + 5) * g.sx;
+    const long long narr = SAMS_NFIELDS + NSCRATCH;
+    const size_t abytes = (size_t)narr * (size_t)g.nelem * sizeof(double);
+    if ((rc = check(cudaMalloc(&arena_, abytes), "cudaMalloc(state)"))) return rc;
+    if ((rc = check(cudaMemsetAsync(arena_, 0, abytes, stream_), "cudaMemset(state)"))) return rc;
+    for (int f = 0; f < SAMS_NFIELDS; ++f) ctx_.f[f] = arena_ + (size_t)f * g.nelem;
+    for (int s = 0; s < NSCRATCH; ++s) ctx_.s[s] = arena_ + (size_t)(SAMS_NFIELDS + s) * g.nelem;
+
+    // 1-D spacings: dxb, dyb, dzb, dxc, dyc, dzc, each (n + 6) long.
+    std::vector<double> dxb, dyb, dzb, dxc, dyc, dzc;
+    axis_host(p.x_min, p.x_max, p.nx, dxb, dxc);
+    axis_host(p.y_min, p.y_max, p.ny, dyb, dyc);
+    axis_host(p.z_min, p.z_max, p.nz, dzb, dzc);
+    std::vector<double> packed;
+    for (auto *v : {&dxb, &dyb, &dzb, &dxc, &dyc, &dzc}) packed.insert(packed.end(), v->begin(), v->end());
+    if ((rc = check(cudaMalloc(&axes_, packed.size() * sizeof(double)), "cudaMalloc(axes)"))) return rc;
+    if ((rc = check(cudaMemcpy(axes_, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice), "axes upload"))) return rc;
+    size_t off = 0;
+    const double **slots[6] = {&ctx_.ax.dxb, &ctx_.ax.dyb, &ctx_.ax.dzb, &ctx_.ax.dxc, &ctx_.ax.dyc, &ctx_.ax.dzc};
+    const size_t lens[6] = {dxb.size(), dyb.size(), dzb.size(), dxc.size(), dyc.size(), dzc.size()};
+    for (int a = 0; a < 6; ++a) {
+        *slots[a] = axes_ + off;
+        off += lens[a];
+    }
+
+    ctx_.p.gamma = p.gas_gamma;
+    ctx_.p.mu0 = p.mu0;
+    ctx_.p.visc1 = p.visc1;
+    ctx_.p.visc2_norm = 0.25 * (p.gas_gamma + 1.0) * p.visc2;  // lagran.cpp:178
+    ctx_.p.dt_multiplier = p.dt_multiplier;
+    ctx_.p.eta_bg = p.eta_background;
+    ctx_.p.eta0 = p.eta0;
+    ctx_.p.j_max = p.j_max;
+
+    if ((rc = check(cudaMalloc(&sc_, sizeof(Scalars)), "cudaMalloc(scalars)"))) return rc;
+    Scalars s0{};
+    s0.dt = 0.0;  // value-initialised runner data: the first step's viscosity sees dt = 0
+    s0.dtmin_bits = 0x7FEFFFFFFFFFFFFFull;  // DBL_MAX
+    if ((rc = check(cudaMemcpy(sc_, &s0, sizeof(s0), cudaMemcpyHostToDevice), "scalars upload"))) return rc;
+    ctx_.sc = sc_;
+    bytes_ = (long long)abytes + (long long)(packed.size() * sizeof(double)) + (long long)sizeof(Scalars);
+    return check(cudaStreamSynchronize(stream_), "init sync");
+}
+
+int Solver::set_bc(int field, int dim, int edge, int kind, double value)
+{
+    if (field < 0 || field >= SAMS_NFIELDS || dim < 0 || dim > 2 || edge < 0 || edge > 1 || kind < SAMS_BC_NONE ||
+        kind > SAMS_BC_CLAMP) {
+        err = "invalid boundary-condition slot or kind";
+        return SAMS_ERR_INVALID;
+    }
+    bc_.kind[field][dim][edge] = (signed char)kind;
+    bc_.value[field][dim][edge] = value;
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    return SAMS_OK;
+}
+
+int Solver::set_stream(cudaStream_t s)
+{
+    stream_ = s ? s : own_stream_;
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    return SAMS_OK;
+}
+
+int Solver::upload(int field, const double *src, cudaMemcpyKind kind)
+{
+    if (field < 0 || field >= SAMS_NFIELDS || !src) { err = "invalid field or buffer"; return SAMS_ERR_INVALID; }
+    const Geom &g = ctx_.g;
+    // box rows are (nz+5) doubles; device rows are padded to g.sy with the
+    // row starting at offset zoff-2.
+    const size_t w = (size_t)(g.nz + 5) * sizeof(double);
+    const size_t rows = (size_t)(g.nx + 5) * (size_t)(g.ny + 5);
+    double *dst = ctx_.f[field] + (g.zoff - 2);
+    return check(cudaMemcpy2DAsync(dst, (size_t)g.sy * sizeof(double), src, w, w, rows, kind, stream_), "upload");
+}
+
+int Solver::download(int field, double *dst, cudaMemcpyKind kind)
+{
+    if (field < 0 || field >= SAMS_NFIELDS || !dst) { err = "invalid field or buffer"; return SAMS_ERR_INVALID; }
+    const Geom &g = ctx_.g;
+    const size_t w = (size_t)(g.nz + 5) * sizeof(double);
+    const size_t rows = (size_t)(g.nx + 5) * (size_t)(g.ny + 5);
+    const double *src = ctx_.f[field] + (g.zoff - 2);
+    int rc = check(cudaMemcpy2DAsync(dst, w, src, (size_t)g.sy * sizeof(double), w, rows, kind, stream_), "download");
+    if (rc) return rc;
+    return check(cudaStreamSynchronize(stream_), "download sync");
+}
+
+template <class Op>
+void Solver::launch(int arg)
+{
+    int lo[3], hi[3];
+    Op::bounds(ctx_.g, arg, lo, hi);
+    const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(hi[0] - lo[0] + 1));
+    k_op<Op><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+    ++launches_;
+}
+
+bool Solver::all_periodic(unsigned mask) const
+{
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        if (mask & (1u << f))
+            for (int d = 0; d < 3; ++d)
+                for (int e = 0; e < 2; ++e)
+                    if (bc_.kind[f][d][e] != SAMS_BC_PERIODIC) return false;
+    return true;
+}
+
+void Solver::bc_fill(unsigned mask)
+{
+    FieldList fl = make_list(mask);
+    if (fl.n == 0) return;
+    const Geom &g = ctx_.g;
+    if (all_periodic(mask)) {
+        // the largest ghost shell is the all-half-cell one
+        const long long e0 = g.nx + 5, e1 = g.ny + 5, e2 = g.nz + 5;
+        const long long cnt = 5 * e1 * e2 + (long long)g.nx * 5 * e2 + (long long)g.nx * g.ny * 5;
+        dim3 grid((unsigned)ceil_div(cnt, kThreads), (unsigned)fl.n);
+        k_bc_periodic<<<grid, kThreads, 0, stream_>>>(ctx_, fl);
+        ++launches_;
+        (void)e0;
+        return;
+    }
+    for (int d = 0; d < 3; ++d) bc_fill_dim(mask, d);
+}
+
+void Solver::bc_fill_dim(unsigned mask, int d)
+{
+    FieldList fl = make_list(mask);
+    if (fl.n == 0) return;
+    const Geom &g = ctx_.g;
+    const long long ext[3] = {g.nx + 5, g.ny + 5, g.nz + 5};
+    long long slab = 3;
+    for (int q = 0; q < 3; ++q)
+        if (q != d) slab *= ext[q];
+    dim3 grid((unsigned)ceil_div(slab, kThreads), (unsigned)fl.n);
+    for (int e = 0; e < 2; ++e) {
+        k_bc_edge<<<grid, kThreads, 0, stream_>>>(ctx_, fl, bc_, d, e);
+        ++launches_;
+    }
+}
+
+void Solver::enqueue_step()
+{
+    const int resistive = p_.resistive_mhd ? 1 : 0;
+    // ---- Lagrangian predictor ----
+    launch<ops::CellPrep>(resistive);
+    launch<ops::NodePrep>(0);
+    launch<ops::Alpha>(0);
+    {
+        int lo[3], hi[3];
+        ops::Visc::bounds(ctx_.g, 0, lo, hi);
+        const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+        const int ni = hi[0] - lo[0] + 1;
+        dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(ni < 16 ? ni : 16));
+        k_visc<<<grid, kThreads, 0, stream_>>>(ctx_);
+        ++launches_;
+    }
+    k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);
+    ++launches_;
+    if (resistive) {
+        for (int sub = 0; sub < 2; ++sub) {
+            launch<ops::ResistRK>(0);
+            launch<ops::ResistB>(sub == 1 ? 1 : 0);
+            bc_fill(FM_BFIELD | FM_ENERGY);
+        }
+    }
+    launch<ops::Pred1>(resistive);
+    launch<ops::Pred2>(0);
+    bc_fill(FM_REMAPV);
+    // ---- corrector ----
+    launch<ops::Corr1>(0);
+    launch<ops::Corr2>(0);
+    bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY);
+    // ---- remap ----
+    launch<ops::BScale>(0);
+    launch<ops::SweepVol<0>>(0);
+    launch<ops::SweepCvc>(0);
+    launch<ops::SweepCT<0>>(0);
+    launch<ops::SweepCTUpd<0>>(0);
+    launch<ops::SweepMass<0>>(0);
+    bc_fill_dim(FM_DM, 0);
+    launch<ops::SweepS6<0>>(0);
+    launch<ops::SweepS7<0>>(0);
+    launch<ops::SweepS8<0>>(0);
+    bc_fill(FM_ALL9);
+    launch<ops::SweepVol<1>>(0);
+    launch<ops::SweepCvc>(0);
+    launch<ops::SweepCT<1>>(0);
+    launch<ops::SweepCTUpd<1>>(0);
+    launch<ops::SweepMass<1>>(0);
+    bc_fill_dim(FM_DM, 1);
+    launch<ops::SweepS6<1>>(0);
+    launch<ops::SweepS7<1>>(0);
+    launch<ops::SweepS8<1>>(0);
+    bc_fill(FM_ALL9);
+    launch<ops::SweepVol<2>>(0);
+    launch<ops::SweepCvc>(0);
+    launch<ops::SweepCT<2>>(0);
+    launch<ops::SweepCTUpd<2>>(0);
+    launch<ops::SweepMass<2>>(0);
+    bc_fill_dim(FM_DM, 2);
+    launch<ops::SweepS6<2>>(0);
+    launch<ops::SweepS7<2>>(0);
+    launch<ops::SweepS8<2>>(0);
+    bc_fill(FM_ALL9);
+    launch<ops::BScale>(1);
+    bc_fill(FM_BFIELD);
+}
+
+int Solver::step(long long nsteps)
+{
+    if (nsteps < 0) { err = "negative step count"; return SAMS_ERR_INVALID; }
+    int rc;
+    if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
+    for (long long s = 0; s < nsteps; ++s) {
+        long long before = launches_;
+        enqueue_step();
+        launches_per_step_ = launches_ - before;
+        if ((rc = check(cudaGetLastError(), "step launch"))) return rc;
+    }
+    return SAMS_OK;
+}
+
+int Solver::step_graph(long long nsteps)
+{
+    if (nsteps < 0) { err = "negative step count"; return SAMS_ERR_INVALID; }
+    if (nsteps == 0) return SAMS_OK;
+    int rc;
+    if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
+    auto it = graphs_.find(nsteps);
+    if (it == graphs_.end()) {
+        cudaGraph_t graph;
+        if ((rc = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture"))) return rc;
+        for (long long s = 0; s < nsteps; ++s) {
+            long long before = launches_;
+            enqueue_step();
+            launches_per_step_ = launches_ - before;
+        }
+        if ((rc = check(cudaStreamEndCapture(stream_, &graph), "end capture"))) return rc;
+        cudaGraphExec_t exec;
+        rc = check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+        cudaGraphDestroy(graph);
+        if (rc) return rc;
+        it = graphs_.emplace(nsteps, exec).first;
+    }
+    return check(cudaGraphLaunch(it->second, stream_), "graph launch");
+}
+
+int Solver::sync()
+{
+    int rc = check(cudaStreamSynchronize(stream_), "synchronize");
+    if (rc) return rc;
+    Scalars s;
+    if ((rc = scalars(s))) return rc;
+    if (s.status) {
+        err = "the CFL timestep became non-finite or non-positive";
+        return SAMS_ERR_NONFINITE;
+    }
+    return SAMS_OK;
+}
+
+int Solver::scalars(Scalars &out)
+{
+    int rc = check(cudaMemcpyAsync(&out, sc_, sizeof(Scalars), cudaMemcpyDeviceToHost, stream_), "scalars read");
+    if (rc) return rc;
+    return check(cudaStreamSynchronize(stream_), "scalars sync");
+}
+
+}  // namespace sams

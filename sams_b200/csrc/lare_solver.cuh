@@ -1,0 +1,83 @@
+// lare_solver.cuh -- one LARE3D solve resident on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lare_device.cuh"
+#include "sams_lare.h"
+
+namespace sams {
+
+// Boundary conditions of all fields as the kernels read them.
+struct BcTable {
+    signed char kind[SAMS_NFIELDS][3][2];
+    double value[SAMS_NFIELDS][3][2];
+};
+
+// Sets of fields filled together (the LARE3D *_bcs groups,
+// src/PhysicsPackages/LARE/boundary.cpp:27-97).
+enum : unsigned {
+    FM_BFIELD = (1u << SAMS_F_BX) | (1u << SAMS_F_BY) | (1u << SAMS_F_BZ),
+    FM_ENERGY = (1u << SAMS_F_ENERGY_ELECTRON) | (1u << SAMS_F_ENERGY_ION),
+    FM_DENSITY = (1u << SAMS_F_RHO),
+    FM_VELOCITY = (1u << SAMS_F_VX) | (1u << SAMS_F_VY) | (1u << SAMS_F_VZ),
+    FM_REMAPV = (1u << SAMS_F_VX1) | (1u << SAMS_F_VY1) | (1u << SAMS_F_VZ1),
+    FM_DM = (1u << SAMS_F_DM),
+    FM_ALL9 = FM_BFIELD | FM_ENERGY | FM_DENSITY | FM_VELOCITY
+};
+
+class Solver {
+public:
+    Solver() = default;
+    ~Solver();
+    Solver(const Solver &) = delete;
+    Solver &operator=(const Solver &) = delete;
+
+    // Returns a sams_status; on failure err holds the reason.
+    int init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device);
+    int set_bc(int field, int dim, int edge, int kind, double value);
+    int set_stream(cudaStream_t s);
+    int upload(int field, const double *src, cudaMemcpyKind kind);
+    int download(int field, double *dst, cudaMemcpyKind kind);
+    int step(long long nsteps);
+    int step_graph(long long nsteps);
+    int sync();
+    int scalars(Scalars &out);
+    long long device_bytes() const { return bytes_; }
+    long long launches_per_step() const { return launches_per_step_; }
+    const Geom &geom() const { return ctx_.g; }
+    double *field_ptr(int f) const { return ctx_.f[f]; }
+
+    std::string err;
+
+    // Enqueue one step on the current stream (no synchronisation).
+    void enqueue_step();
+
+private:
+    int check(cudaError_t e, const char *what);
+    void bc_fill(unsigned mask);
+    void bc_fill_dim(unsigned mask, int dim);
+    bool all_periodic(unsigned mask) const;
+    template <class Op> void launch(int arg);
+    void free_all();
+
+    sams_lare_params p_{};
+    BcTable bc_{};
+    int device_ = 0;
+    cudaStream_t own_stream_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    Ctx ctx_{};
+    double *arena_ = nullptr;
+    double *axes_ = nullptr;
+    Scalars *sc_ = nullptr;
+    long long bytes_ = 0;
+    long long launches_ = 0;
+    long long launches_per_step_ = 0;
+    std::map<long long, cudaGraphExec_t> graphs_;
+};
+
+}  // namespace sams

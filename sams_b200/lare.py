@@ -1,0 +1,233 @@
+"""Python access to the B200 LARE3D library through its C ABI
+(include/sams_lare.h).
+
+The reference drives LARE3D as a package of a SAMS::runner
+(src/PhysicsPackages/LARE/shared_data.h:229-508); here a :class:`LARE3D`
+object owns one GPU-resident solve and exposes the same life cycle: set up
+parameters and boundary conditions, fill the initial state, step, read the
+state back.  All arithmetic happens in libsams_lare.so on the GPU; there is
+no CPU fallback, and constructing a solver without the library or without a
+GPU raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libsams_lare.so")
+
+NFIELDS = 13
+FIELD_NAMES = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz",
+               "vx1", "vy1", "vz1", "bx", "by", "bz", "dm"]
+FIELD = {n: i for i, n in enumerate(FIELD_NAMES)}
+STAGGER = [(0, 0, 0)] * 3 + [(1, 1, 1)] * 6 + [(1, 0, 0), (0, 1, 0), (0, 0, 1), (0, 0, 0)]
+BC = {"none": 0, "periodic": 1, "zero_gradient": 2, "mirror": 3, "clamp": 4}
+CASES = {"ot": 0, "rf": 1, "harris": 2}
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "out of memory", -3: "CUDA error",
+          -4: "unsupported option", -5: "non-finite timestep", -6: "timeout", -7: "over budget"}
+
+
+class Params(ctypes.Structure):
+    """sams_lare_params (include/sams_lare_layout.h)."""
+    _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("nz", ctypes.c_int64),
+                ("x_min", ctypes.c_double), ("x_max", ctypes.c_double),
+                ("y_min", ctypes.c_double), ("y_max", ctypes.c_double),
+                ("z_min", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("gas_gamma", ctypes.c_double), ("mu0", ctypes.c_double),
+                ("visc1", ctypes.c_double), ("visc2", ctypes.c_double),
+                ("dt_multiplier", ctypes.c_double),
+                ("eta_background", ctypes.c_double), ("eta0", ctypes.c_double),
+                ("j_max", ctypes.c_double),
+                ("resistive_mhd", ctypes.c_int32), ("rke", ctypes.c_int32),
+                ("geometry", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Bcs(ctypes.Structure):
+    """sams_lare_bcs: one condition per (field, dim, edge)."""
+    _fields_ = [("kind", ctypes.c_int32 * 2 * 3 * NFIELDS),
+                ("value", ctypes.c_double * 2 * 3 * NFIELDS)]
+
+
+class LareError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+_P = ctypes.POINTER(ctypes.c_double)
+
+
+def lib():
+    """Load libsams_lare.so (building it first if this checkout has no
+    built copy and nvcc is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    i64 = ctypes.c_int64
+    L.sams_lare_last_error.restype = ctypes.c_char_p
+    L.sams_lare_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(Bcs), ctypes.c_int, ctypes.POINTER(vp)]
+    L.sams_lare_destroy.argtypes = [vp]
+    L.sams_lare_set_stream.argtypes = [vp, vp]
+    L.sams_lare_set_bc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    L.sams_lare_upload_field.argtypes = [vp, ctypes.c_int, _P]
+    L.sams_lare_download_field.argtypes = [vp, ctypes.c_int, _P]
+    L.sams_lare_upload_field_device.argtypes = [vp, ctypes.c_int, vp]
+    L.sams_lare_download_field_device.argtypes = [vp, ctypes.c_int, vp]
+    L.sams_lare_step.argtypes = [vp, i64]
+    L.sams_lare_step_graph.argtypes = [vp, i64]
+    L.sams_lare_synchronize.argtypes = [vp]
+    L.sams_lare_get_dt.argtypes = [vp, _P]
+    L.sams_lare_get_time.argtypes = [vp, _P]
+    L.sams_lare_get_step.argtypes = [vp, ctypes.POINTER(i64)]
+    L.sams_lare_field_device_ptr.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(i64),
+                                             ctypes.POINTER(i64)]
+    L.sams_lare_device_bytes.argtypes = [vp, ctypes.POINTER(i64)]
+    L.sams_lare_launches_per_step.argtypes = [vp, ctypes.POINTER(i64)]
+    L.sams_lare_case_setup.argtypes = [ctypes.c_int, i64, i64, i64, ctypes.c_double,
+                                       ctypes.POINTER(Params), ctypes.POINTER(Bcs)]
+    L.sams_lare_case_fields.argtypes = [ctypes.c_int, ctypes.POINTER(Params), ctypes.c_uint64, ctypes.c_double,
+                                        ctypes.POINTER(_P)]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise LareError(rc, lib().sams_lare_last_error().decode())
+
+
+def box_shape(nx, ny, nz):
+    return (nx + 5, ny + 5, nz + 5)
+
+
+def field_slices(field, nx, ny, nz):
+    """Box slices covering a field's own local range."""
+    idx = FIELD[field] if isinstance(field, str) else field
+    return tuple(slice(0 if s else 1, n + 5) for s, n in zip(STAGGER[idx], (nx, ny, nz)))
+
+
+def case_setup(case, nx, ny, nz, b0=0.0):
+    """Parameters and boundary conditions of a named workload."""
+    p, b = Params(), Bcs()
+    _check(lib().sams_lare_case_setup(CASES.get(case, case), nx, ny, nz, b0, ctypes.byref(p), ctypes.byref(b)))
+    return p, b
+
+
+def case_fields(case, params, seed=1, b0=0.0):
+    """Initial state of a named workload as 13 box arrays."""
+    shape = box_shape(params.nx, params.ny, params.nz)
+    arrs = [np.zeros(shape) for _ in range(NFIELDS)]
+    ptrs = (_P * NFIELDS)(*[a.ctypes.data_as(_P) for a in arrs])
+    _check(lib().sams_lare_case_fields(CASES.get(case, case), ctypes.byref(params), seed, b0, ptrs))
+    return arrs
+
+
+class LARE3D:
+    """One LARE3D solve resident on a GPU (the reference package's name and
+    role, shared_data.h:330-345)."""
+
+    name = "LARE3D"
+    coreSimulation = True
+    timeSimulation = True
+
+    def __init__(self, params, bcs, device=0):
+        self.params = params
+        self.shape = box_shape(params.nx, params.ny, params.nz)
+        h = ctypes.c_void_p()
+        _check(lib().sams_lare_create(ctypes.byref(params), ctypes.byref(bcs), device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sams_lare_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_bc(self, field, dim, edge, kind, value=0.0):
+        f = FIELD[field] if isinstance(field, str) else field
+        k = BC[kind] if isinstance(kind, str) else kind
+        _check(lib().sams_lare_set_bc(self._h, f, dim, edge, k, value))
+
+    def upload(self, field, arr):
+        f = FIELD[field] if isinstance(field, str) else field
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self.shape:
+            raise ValueError(f"expected box shape {self.shape}, got {a.shape}")
+        _check(lib().sams_lare_upload_field(self._h, f, a.ctypes.data_as(_P)))
+        _check(lib().sams_lare_synchronize(self._h))
+
+    def upload_all(self, fields):
+        for f, a in enumerate(fields):
+            self.upload(f, a)
+
+    def download(self, field, out=None):
+        f = FIELD[field] if isinstance(field, str) else field
+        if out is None:
+            out = np.empty(self.shape)
+        _check(lib().sams_lare_download_field(self._h, f, out.ctypes.data_as(_P)))
+        return out
+
+    def step(self, n=1, graph=False):
+        if graph:
+            _check(lib().sams_lare_step_graph(self._h, n))
+        else:
+            _check(lib().sams_lare_step(self._h, n))
+
+    def synchronize(self):
+        _check(lib().sams_lare_synchronize(self._h))
+
+    @property
+    def dt(self):
+        v = ctypes.c_double()
+        _check(lib().sams_lare_get_dt(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def time(self):
+        v = ctypes.c_double()
+        _check(lib().sams_lare_get_time(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def steps(self):
+        v = ctypes.c_int64()
+        _check(lib().sams_lare_get_step(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def device_bytes(self):
+        v = ctypes.c_int64()
+        _check(lib().sams_lare_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def launches_per_step(self):
+        v = ctypes.c_int64()
+        _check(lib().sams_lare_launches_per_step(self._h, ctypes.byref(v)))
+        return v.value
+
+    def set_stream(self, stream_ptr):
+        _check(lib().sams_lare_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

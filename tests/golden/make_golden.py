@@ -1,0 +1,63 @@
+"""Generate the golden fixtures in this directory from the REFERENCE itself.
+
+Runs oracle/_ref/lare_ref (the unmodified reference LARE3D sources compiled
+by oracle/Makefile, driven by its own SAMS::runner) on small seeded cases and
+stores, per case, the nine state fields over their own index ranges plus the
+dt history.  The reference tree is needed only to (re)generate; the .npz
+files are committed and used by tests on machines without it.
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import lare_oracle as lo  # noqa: E402
+from oracle.dumpio import Dump  # noqa: E402
+
+# (name, case, nx, ny, nz, steps, seed, b0)
+CASES = [
+    ("ot_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0),
+    ("ot_7x5x3_s3", "ot", 7, 5, 3, 3, 1, 0.0),
+    ("ot_b0_10x10x4_s4", "ot", 10, 10, 4, 4, 1, 0.9 / (4 * np.pi) ** 0.5),
+    ("rf_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0),
+    ("harris_12x10x6_s4", "harris", 12, 10, 6, 4, 3, 0.0),
+]
+STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
+
+
+def main():
+    lo.build()
+    if not os.path.exists(lo.REF_BIN):
+        raise SystemExit("reference harness not built (needs the reference tree)")
+    for name, case, nx, ny, nz, steps, seed, b0 in CASES:
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "d.dump")
+            summary = lo.run_reference(case, nx, ny, nz, steps, path, seed=seed, b0=b0)
+            d = Dump(path)
+            out = {}
+            for f in STATE:
+                out[f] = d.box(f)
+            out["dts"] = np.array(d.header["dts"])
+            meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0,
+                        time=summary["time"], generator="oracle/_ref/lare_ref (reference LARE3D)")
+            out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+            print(name, "dt", d.header["dt"])
+
+
+def load(name):
+    z = np.load(os.path.join(HERE, name + ".npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    return z, meta
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,118 @@
+"""GPU timestep (libsams_lare.so through its C ABI) against the reference.
+
+Bit-for-bit against the reference's own outputs (tests/golden, made by the
+compiled reference) and against the CPU checker at further sizes; at the
+benchmark's full size through properties that do not depend on size (mass
+conservation on a periodic grid, run-to-run determinism, graph == stream).
+"""
+import numpy as np
+import pytest
+
+from sams_b200 import lare
+from tests.golden.make_golden import CASES, STATE, load
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(case, nx, ny, nz, seed=1, b0=0.0):
+    p, b = lare.case_setup(case, nx, ny, nz, b0)
+    s = lare.LARE3D(p, b)
+    s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
+    return s
+
+
+def _assert_state_equal(s, ref_field, label):
+    for f in STATE:
+        ref = ref_field(f)
+        m = ~np.isnan(ref)
+        got = s.download(f)
+        if not np.array_equal(got[m], ref[m]):
+            diff = np.abs(got[m] - ref[m])
+            rel = diff.max() / max(np.abs(ref[m]).max(), 1e-300)
+            raise AssertionError(f"{label}: {f} differs, max abs {diff.max():.3e}, rel {rel:.3e}")
+
+
+@pytest.mark.parametrize("name", [c[0] for c in CASES])
+def test_gpu_matches_reference_golden(name):
+    z, meta = load(name)
+    s = _solver(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["seed"], meta["b0"])
+    dts = []
+    for _ in range(meta["steps"]):
+        s.step(1)
+        dts.append(s.dt)
+    assert np.array_equal(np.array(dts), z["dts"]), (dts, z["dts"])
+    _assert_state_equal(s, lambda f: z[f], name)
+    assert s.steps == meta["steps"]
+    assert s.time == pytest.approx(meta["time"], rel=0, abs=0)
+
+
+@pytest.mark.parametrize("case,n,steps", [
+    ("ot", (24, 20, 8), 30),
+    ("ot", (33, 17, 5), 10),
+    ("rf", (16, 16, 16), 10),
+    ("rf", (20, 12, 9), 6),
+    ("harris", (24, 16, 8), 10),
+])
+def test_gpu_matches_checker(case, n, steps, oracle_lib):
+    lo = oracle_lib
+    nx, ny, nz = n
+    s = _solver(case, nx, ny, nz, seed=9)
+    p, b = lo.case_setup(case, nx, ny, nz)
+    o = lo.Oracle(p, b, lo.case_fields(case, p, seed=9))
+    for _ in range(steps):
+        s.step(1)
+        o.step(1)
+        assert s.dt == o.dt
+    _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"{case}{n}")
+
+
+def _masked(box, f, nx, ny, nz):
+    out = np.full(box.shape, np.nan)
+    sl = lare.field_slices(f, nx, ny, nz)
+    out[sl] = box[sl]
+    return out
+
+
+def test_gpu_matches_checker_64cube_resistive(oracle_lib):
+    lo = oracle_lib
+    s = _solver("rf", 64, 64, 64, seed=2)
+    p, b = lo.case_setup("rf", 64, 64, 64)
+    o = lo.Oracle(p, b, lo.case_fields("rf", p, seed=2))
+    s.step(4)
+    o.step(4)
+    assert s.dt == o.dt
+    _assert_state_equal(s, lambda f: _masked(o.field(f), f, 64, 64, 64), "rf64")
+
+
+def test_graph_equals_stream_and_is_deterministic():
+    a = _solver("ot", 32, 32, 4)
+    b = _solver("ot", 32, 32, 4)
+    a.step(12)
+    b.step(12, graph=True)
+    a.synchronize()
+    b.synchronize()
+    for f in STATE:
+        assert np.array_equal(a.download(f), b.download(f)), f
+    assert a.dt == b.dt and a.time == b.time
+
+
+def test_full_size_256_cube_conserves_mass_and_is_deterministic():
+    """The benchmark configuration (256^3 random field, resistive) at full
+    size: total mass sum(rho * cv) over the periodic domain is conserved to
+    1e-13 relative, and two solves from the same state agree bit for bit."""
+    n = 256
+    p, b = lare.case_setup("rf", n, n, n)
+    fields = lare.case_fields("rf", p, seed=1)
+    cv = (1.0 / n) ** 3
+    m0 = fields[0][3:n + 3, 3:n + 3, 3:n + 3].sum() * cv
+    runs = []
+    for _ in range(2):
+        s = lare.LARE3D(p, b)
+        s.upload_all(fields)
+        s.step(3, graph=True)
+        s.synchronize()
+        runs.append(s.download("rho"))
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
+    m1 = runs[0][3:n + 3, 3:n + 3, 3:n + 3].sum() * cv
+    assert abs(m1 - m0) / m0 < 1e-13

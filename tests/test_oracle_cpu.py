@@ -1,0 +1,81 @@
+"""The CPU checker (oracle/lare_oracle.c) against the reference.
+
+Golden fixtures in tests/golden/ were produced by the reference itself
+(tests/golden/make_golden.py runs the compiled reference LARE3D); where the
+reference binary is present (this build container) the checker is also
+compared with it directly on further cases.  The bar is bit-for-bit.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import lare_oracle as lo
+from tests.golden.make_golden import CASES, STATE, load
+
+
+def _run_checker(case, nx, ny, nz, steps, seed, b0):
+    p, b = lo.case_setup(case, nx, ny, nz, b0)
+    o = lo.Oracle(p, b, lo.case_fields(case, p, seed=seed, b0=b0))
+    dts = []
+    for _ in range(steps):
+        o.step(1)
+        dts.append(o.dt)
+    return o, dts
+
+
+@pytest.mark.parametrize("name", [c[0] for c in CASES])
+def test_checker_matches_reference_golden(name, oracle_lib):
+    z, meta = load(name)
+    o, dts = _run_checker(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["steps"], meta["seed"], meta["b0"])
+    assert np.array_equal(np.array(dts), z["dts"]), "dt history differs"
+    for f in STATE:
+        ref = z[f]
+        m = ~np.isnan(ref)
+        got = o.field(f)
+        assert np.array_equal(got[m], ref[m]), f"{name}: field {f} differs (max {np.abs(got[m]-ref[m]).max()})"
+
+
+@pytest.mark.skipif(not os.path.exists(lo.REF_BIN), reason="reference harness binary not built here")
+@pytest.mark.parametrize("case,n,steps", [("ot", (9, 11, 5), 12), ("rf", (8, 8, 8), 6), ("harris", (10, 8, 4), 6)])
+def test_checker_matches_reference_binary(case, n, steps, tmp_path, oracle_lib):
+    from oracle.dumpio import Dump
+    nx, ny, nz = n
+    dump = str(tmp_path / "ref.dump")
+    lo.run_reference(case, nx, ny, nz, steps, dump, seed=11)
+    d = Dump(dump)
+    o, dts = _run_checker(case, nx, ny, nz, steps, 11, 0.0)
+    assert dts == d.header["dts"]
+    for f in lo.FIELD_NAMES:
+        ref = d.box(f)
+        m = ~np.isnan(ref)
+        assert np.array_equal(o.field(f)[m], ref[m]), f
+    # grid metrics as LARE3D::grid builds them
+    for name in ["cv", "cvc", "dxab", "dyab", "dzab", "dxac", "dyac", "dzac"]:
+        ref = d.box(name)
+        m = ~np.isnan(ref)
+        assert np.array_equal(o.named(name)[m], ref[m]), name
+
+
+def test_planted_error_is_caught(oracle_lib):
+    """A mistake planted in the checker's input state must show up in the
+    comparison (guards against a vacuous test)."""
+    z, meta = load("ot_12x10x6_s5")
+    p, b = lo.case_setup("ot", meta["nx"], meta["ny"], meta["nz"])
+    fields = lo.case_fields("ot", p)
+    fields[0][7, 7, 4] *= 1.0 + 1e-12
+    o = lo.Oracle(p, b, fields)
+    o.step(meta["steps"])
+    ref = z["rho"]
+    m = ~np.isnan(ref)
+    assert not np.array_equal(o.field("rho")[m], ref[m])
+
+
+def test_periodic_mass_conservation_checker(oracle_lib):
+    p, b = lo.case_setup("ot", 16, 16, 4)
+    o = lo.Oracle(p, b, lo.case_fields("ot", p))
+    cv = o.named("cv")[3:-2, 3:-2, 3:-2]
+    m0 = (o.field("rho")[3:-2, 3:-2, 3:-2] * cv).sum()
+    o.step(20)
+    m1 = (o.field("rho")[3:-2, 3:-2, 3:-2] * cv).sum()
+    assert abs(m1 - m0) / m0 < 1e-13
