@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LARE3D timestep (one JSON line on rank 0).
+
+Workload: the plain 256^3 periodic random-field cube (resistive MHD,
+eta = 1e-4, seeded initial state), FP64.  A "step" is one full LARE3D
+timestep (Lagrangian predictor + corrector + x/y/z remap) of that cube.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`value` is device-timed throughput in cell-updates/s with the state resident
+in HBM; `e2e` is the same solve through the C ABI from pinned host buffers
+(state upload, K steps each reading back dt, state download).  Under torchrun
+every rank runs its own independent solve (replicas; the path does not shard
+within a solve), time = max over ranks.  `--impl reference` times the
+reference LARE3D CPU code (oracle/_ref/lare_ref_bench, built from the
+reference sources) on this host's cores for the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-updates/s plain vs batched (1 B200, 1e-10 rel); p50/p99 solve latency"
+UNIT = "cell-updates/s"
+# Compulsory FP64 HBM traffic of one resistive cell-update: state read/write
+# per phase, 8 B per value (dt pass 72, predictor 96, corrector 144, three
+# sweeps 3 x 176, two resistive sub-steps 2 x 72).
+ALGO_BYTES_PER_CELL_UPDATE = 984
+WORKLOAD = ("plain LARE3D step, 256^3 periodic random-field cube [0,1]^3, rho=1, p=0.1, "
+            "|B|rms=0.1, |v|rms=0.05, k=1..8, gamma=5/3, eta=1e-4 (resistive), seeded synthetic IC")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sams", choices=["sams", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if args.impl == "sams":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(n):
+    """DRAM bytes per step from the committed ncu summary of this workload,
+    if one exists (profiles/lare_step_rf256_traffic.json)."""
+    path = os.path.join(ROOT, "profiles", f"lare_step_rf{n}_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)["dram_bytes_per_step"]
+    except Exception:
+        return None
+
+
+def cpu_reference(n, steps, threads=None):
+    """Time the reference LARE3D CPU code (or, without its binary, the C
+    restatement) on this host for `steps` steps of the n^3 workload."""
+    from oracle import lare_oracle as lo
+    threads = threads or os.cpu_count()
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
+    if os.path.exists(lo.REF_BENCH_BIN):
+        cmd = [lo.REF_BENCH_BIN, "--case", "rf", "--nx", str(n), "--ny", str(n), "--nz", str(n),
+               "--steps", str(steps), "--seed", "1", "--quiet"]
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
+        rec = json.loads(out.strip().splitlines()[-1])
+        return rec["step_seconds"], "reference", threads
+    # the C restatement (ctypes, OpenMP)
+    p, b = lo.case_setup("rf", n, n, n)
+    o = lo.Oracle(p, b, lo.case_fields("rf", p, seed=1))
+    secs = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        o.step(1)
+        secs.append(time.perf_counter() - t0)
+    return secs, "port", threads
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    n = args.n
+    total = args.warmup + args.steps
+    secs, kind, threads = cpu_reference(n, total)
+    timed = secs[args.warmup:]
+    cells = float(n) ** 3
+    value = cells * len(timed) / sum(timed)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "case": "rf", "grid": [n, n, n], "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{len(timed)} timed steps of the {n}^3 workload after {args.warmup} warm-up steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_sams(args, world, rank, local, pg):
+    import torch
+    from sams_b200 import lare
+
+    torch.cuda.set_device(local)
+    n = args.n
+    cells = float(n) ** 3
+    p, b = lare.case_setup("rf", n, n, n)
+    fields = lare.case_fields("rf", p, seed=1 + rank)
+    # a dedicated stream: the solver launches on it and the events bracket it
+    stream = torch.cuda.Stream(device=local)
+
+    # ---------------- device-resident throughput ----------------
+    s = lare.LARE3D(p, b, device=local)
+    s.set_stream(stream.cuda_stream)
+    s.upload_all(fields)
+    for _ in range(args.warmup):
+        s.step(1, graph=True)
+    s.synchronize()
+    launches = s.launches_per_step
+    if pg is not None:
+        pg.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.step(1, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    s.synchronize()
+    ms_per_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3)
+    phases = s.phase_times()
+    s.synchronize()
+    s.close()
+
+    # ---------------- end to end through the C ABI ----------------
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(fields[f]).pin_memory() for f in range(lare.NFIELDS)]
+        state = [f for f in range(lare.NFIELDS) if lare.FIELD_NAMES[f] in
+                 ("rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz")]
+        outs = [torch.empty_like(pinned[f]).pin_memory() for f in state]
+        s2 = lare.LARE3D(p, b, device=local)
+        s2.set_stream(stream.cuda_stream)
+        s2.upload_all(fields)              # the solve's scratch/aux fields
+        s2.step(1, graph=True)             # graph recorded outside the timed region
+        s2.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        L = lare.lib()
+        h = s2.handle
+        e0.record(stream)
+        for f in state:
+            lare._check(L.sams_lare_upload_field(h, f, ctypes_addr(pinned[f])))
+        dts = []
+        for _ in range(args.steps):
+            lare._check(L.sams_lare_step_graph(h, 1))
+            dts.append(s2.dt)
+        for f, o in zip(state, outs):
+            lare._check(L.sams_lare_download_field(h, f, ctypes_addr(o)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if pg is not None:
+            t = torch.tensor([ems], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ems = float(t.item())
+        box_bytes = int(np.prod(lare.box_shape(n, n, n))) * 8
+        e2e = {"value": world * cells * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": len(state) * box_bytes / args.steps,
+               "d2h_bytes_per_step": (len(state) * box_bytes + 8 * args.steps) / args.steps,
+               "what": "state upload from pinned host memory, K steps each reading dt back, state download"}
+        s2.close()
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    achieved = ALGO_BYTES_PER_CELL_UPDATE * cells / (ms_per_step / 1e3) / 1e9
+    traffic = ncu_traffic(n)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "one LARE3D timestep (a CUDA graph of %d kernels)" % launches,
+                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL_UPDATE * cells}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            csteps = 4 if n >= 256 else 8
+            secs, kind, threads = cpu_reference(n, csteps)
+            cpu = {"value": cells * len(secs) / sum(secs), "unit": UNIT, "cores": threads, "kind": kind,
+                   "sample": f"{csteps} steps of the {n}^3 workload (all steps timed)"}
+        except Exception as ex:  # report, do not fail the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "case": "rf", "grid": [n, n, n],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (each field 144 MB, 32 x 144 MB resident)"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": launches * args.steps,
+        "phases_ms": dict(zip(["lagrangian", "corrector", "remap_x", "remap_y", "remap_z"], phases)),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ctypes_addr(t):
+    import ctypes
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), ctypes.POINTER(ctypes.c_double))
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_sams(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -107,6 +107,12 @@ int sams_lare_field_device_ptr(sams_lare_solver *h, int field, double **ptr,
 /* Device bytes held by the solver. */
 int sams_lare_device_bytes(sams_lare_solver *h, int64_t *bytes);
 
+/* Advance one step and report the device time (ms) of its five phases:
+ * Lagrangian predictor (startOfTimestep), corrector (halfTimestep), and the
+ * x, y and z remap sweeps (endOfTimestep).  Replaces the reference's
+ * per-event timers (include/runner/runnerMacros.h:113-150). */
+int sams_lare_phase_times(sams_lare_solver *h, double ms[5]);
+
 /* Number of kernel launches one sams_lare_step(h, 1) issues. */
 int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches);
 

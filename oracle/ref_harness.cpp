@@ -48,7 +48,8 @@ namespace oracle
         int dump_phase = 0;     // 0 start, 1 half, 2 end
         sams_lare_params params{};
         sams_lare_bcs bcs{};
-        std::vector<double> dts, times;
+        std::vector<double> dts, times, step_seconds;
+        std::chrono::steady_clock::time_point last_mark;
         bool dumped = false;
     };
     config g;
@@ -300,6 +301,9 @@ namespace oracle
         void halfTimestep(LARE::simulationData &data) { maybeDump(data, 1, 0.0); }
         void endOfTimestep(LARE::simulationData &data)
         {
+            auto now = std::chrono::steady_clock::now();
+            g.step_seconds.push_back(std::chrono::duration<double>(now - g.last_mark).count());
+            g.last_mark = now;
             ++localStep;
             g.dts.push_back(data.dt);
             maybeDump(data, 2, 0.0);
@@ -384,6 +388,7 @@ int main(int argc, char *argv[])
 
         auto &t = std::get<SAMS::timeState>(runner.runnerData);
         auto t0 = std::chrono::steady_clock::now();
+        g.last_mark = t0;
         if (g.steps > 0)
         {
             // runner::runPackages step loop (runner.h:564-586) without output
@@ -404,10 +409,17 @@ int main(int argc, char *argv[])
         if (!dumpFinal.empty()) writeDump(dumpFinal, data, t.step, t.time, "final");
         double cells = double(g.nx) * double(g.ny) * double(g.nz);
         std::cout.clear();
+        std::string st;
+        for (size_t i = 0; i < g.step_seconds.size(); ++i)
+        {
+            char buf[64];
+            std::snprintf(buf, sizeof buf, "%s%.6f", i ? "," : "", g.step_seconds[i]);
+            st += buf;
+        }
         std::printf("{\"case\":%d,\"nx\":%lld,\"ny\":%lld,\"nz\":%lld,\"steps\":%lld,\"loop_s\":%.6f,"
-                    "\"cell_updates_per_s\":%.6e,\"threads\":%d,\"time\":%.17g,\"dt\":%.17g}\n",
+                    "\"cell_updates_per_s\":%.6e,\"threads\":%d,\"time\":%.17g,\"dt\":%.17g,\"step_seconds\":[%s]}\n",
                     g.case_id, (long long)g.nx, (long long)g.ny, (long long)g.nz, (long long)steps_done, loop_s,
-                    loop_s > 0 ? cells * double(steps_done) / loop_s : 0.0, omp_get_max_threads(), t.time, t.dt);
+                    loop_s > 0 ? cells * double(steps_done) / loop_s : 0.0, omp_get_max_threads(), t.time, t.dt, st.c_str());
         runner.finalizePackages();
     }
     portableWrapper::finalize();

@@ -167,6 +167,12 @@ int sams_lare_device_bytes(sams_lare_solver *h, int64_t *bytes)
     return SAMS_OK;
 }
 
+int sams_lare_phase_times(sams_lare_solver *h, double ms[5])
+{
+    if (!h || !ms) return fail(SAMS_ERR_INVALID, "invalid argument");
+    return pass(h, h->s.phase_times(ms));
+}
+
 int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches)
 {
     if (!h || !launches) return fail(SAMS_ERR_INVALID, "invalid argument");

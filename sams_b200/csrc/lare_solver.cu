@@ -449,9 +449,13 @@ void Solver::bc_fill_dim(unsigned mask, int d)
     }
 }
 
-void Solver::enqueue_step()
+void Solver::enqueue_step(cudaEvent_t *marks)
 {
     const int resistive = p_.resistive_mhd ? 1 : 0;
+    auto mark = [&](int m) {
+        if (marks) cudaEventRecord(marks[m], stream_);
+    };
+    mark(0);
     // ---- Lagrangian predictor ----
     launch<ops::CellPrep>(resistive);
     launch<ops::NodePrep>(0);
@@ -477,10 +481,12 @@ void Solver::enqueue_step()
     launch<ops::Pred1>(resistive);
     launch<ops::Pred2>(0);
     bc_fill(FM_REMAPV);
+    mark(1);
     // ---- corrector ----
     launch<ops::Corr1>(0);
     launch<ops::Corr2>(0);
     bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY);
+    mark(2);
     // ---- remap ----
     launch<ops::BScale>(0);
     launch<ops::SweepVol<0>>(0);
@@ -493,6 +499,7 @@ void Solver::enqueue_step()
     launch<ops::SweepS7<0>>(0);
     launch<ops::SweepS8<0>>(0);
     bc_fill(FM_ALL9);
+    mark(3);
     launch<ops::SweepVol<1>>(0);
     launch<ops::SweepCvc>(0);
     launch<ops::SweepCT<1>>(0);
@@ -503,6 +510,7 @@ void Solver::enqueue_step()
     launch<ops::SweepS7<1>>(0);
     launch<ops::SweepS8<1>>(0);
     bc_fill(FM_ALL9);
+    mark(4);
     launch<ops::SweepVol<2>>(0);
     launch<ops::SweepCvc>(0);
     launch<ops::SweepCT<2>>(0);
@@ -515,6 +523,25 @@ void Solver::enqueue_step()
     bc_fill(FM_ALL9);
     launch<ops::BScale>(1);
     bc_fill(FM_BFIELD);
+    mark(5);
+}
+
+int Solver::phase_times(double ms[5])
+{
+    int rc;
+    if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
+    cudaEvent_t ev[6];
+    for (int i = 0; i < 6; ++i)
+        if ((rc = check(cudaEventCreate(&ev[i]), "cudaEventCreate"))) return rc;
+    enqueue_step(ev);
+    rc = check(cudaEventSynchronize(ev[5]), "phase sync");
+    for (int i = 0; i < 5 && !rc; ++i) {
+        float t = 0.f;
+        rc = check(cudaEventElapsedTime(&t, ev[i], ev[i + 1]), "cudaEventElapsedTime");
+        ms[i] = t;
+    }
+    for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+    return rc;
 }
 
 int Solver::step(long long nsteps)

@@ -54,8 +54,12 @@ public:
 
     std::string err;
 
-    // Enqueue one step on the current stream (no synchronisation).
-    void enqueue_step();
+    // Enqueue one step on the current stream (no synchronisation).  With
+    // marks != nullptr, records marks[0..5] around the step's phases:
+    // Lagrangian predictor, corrector, x, y and z remap sweeps.
+    void enqueue_step(cudaEvent_t *marks = nullptr);
+    // Run one step and return the device time of each phase in ms.
+    int phase_times(double ms[5]);
 
 private:
     int check(cudaError_t e, const char *what);

@@ -91,6 +91,7 @@ def lib():
                                              ctypes.POINTER(i64)]
     L.sams_lare_device_bytes.argtypes = [vp, ctypes.POINTER(i64)]
     L.sams_lare_launches_per_step.argtypes = [vp, ctypes.POINTER(i64)]
+    L.sams_lare_phase_times.argtypes = [vp, _P]
     L.sams_lare_case_setup.argtypes = [ctypes.c_int, i64, i64, i64, ctypes.c_double,
                                        ctypes.POINTER(Params), ctypes.POINTER(Bcs)]
     L.sams_lare_case_fields.argtypes = [ctypes.c_int, ctypes.POINTER(Params), ctypes.c_uint64, ctypes.c_double,
@@ -228,6 +229,13 @@ class LARE3D:
         v = ctypes.c_int64()
         _check(lib().sams_lare_launches_per_step(self._h, ctypes.byref(v)))
         return v.value
+
+    def phase_times(self):
+        """Run one step; device ms of (lagrangian, corrector, remap_x,
+        remap_y, remap_z)."""
+        out = (ctypes.c_double * 5)()
+        _check(lib().sams_lare_phase_times(self._h, out))
+        return list(out)
 
     def set_stream(self, stream_ptr):
         _check(lib().sams_lare_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
