@@ -116,6 +116,25 @@ int sams_lare_phase_times(sams_lare_solver *h, double ms[5]);
 /* Number of kernel launches one sams_lare_step(h, 1) issues. */
 int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches);
 
+/* No counterpart in the reference.  Advance nsteps timesteps of a solve whose
+ * 13 fields live in the caller's own device memory, allocating nothing: for
+ * callers that cannot call cudaMalloc while running (a host code whose device
+ * memory all comes from its own pool, or one that must not grow its device
+ * footprint).  dev_fields[f] are dense box buffers on the current device
+ * (-2..n+2 per dimension, z fastest, no padding), read and written in place.
+ * *dt_inout is the previous step's dt (0 before the first step) and
+ * *time_inout the time; both are updated.  Runs on `stream` (NULL = legacy
+ * default stream) and returns when the steps are done.
+ * The step's scratch is a static 64 MiB device array inside the library
+ * (held by every GPU that loads it until exit), enough for
+ * (nx+5)(ny+5)(nz+5) up to about 440000; larger grids are rejected with
+ * SAMS_ERR_INVALID.  The first call on a device looks up that array's address
+ * and should come before any stream capture.  Calls share the array: calls
+ * that overlap on the GPU race. */
+int sams_lare_step_noalloc(const sams_lare_params *params, const sams_lare_bcs *bcs,
+                           double *const dev_fields[SAMS_NFIELDS], double *dt_inout,
+                           double *time_inout, int64_t nsteps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

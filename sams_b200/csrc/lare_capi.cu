@@ -34,6 +34,13 @@ cudaMemcpyKind host_kind(const void *p)
 }
 }  // namespace
 
+// Library-internal: lets other translation units report through
+// sams_lare_last_error().
+__attribute__((visibility("hidden"))) void sams_capi_set_last_error(const std::string &msg)
+{
+    g_last_error = msg;
+}
+
 extern "C" {
 
 int sams_lare_abi_version(void) { return 100; }

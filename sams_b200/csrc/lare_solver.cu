@@ -348,6 +348,34 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     return check(cudaStreamSynchronize(stream_), "init sync");
 }
 
+int Solver::init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, const Ctx &ctx, int device,
+                          cudaStream_t stream)
+{
+    if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
+    p_ = p;
+    device_ = device;
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 2; ++e) {
+                int k = bcs.kind[f][d][e];
+                if (k < SAMS_BC_NONE || k > SAMS_BC_CLAMP) { err = "unknown boundary-condition kind"; return SAMS_ERR_INVALID; }
+                bc_.kind[f][d][e] = (signed char)k;
+                bc_.value[f][d][e] = bcs.value[f][d][e];
+            }
+    ctx_ = ctx;
+    sc_ = ctx.sc;  // borrowed: release_borrowed() must clear it before destruction
+    stream_ = stream;
+    return SAMS_OK;
+}
+
+void Solver::release_borrowed()
+{
+    sc_ = nullptr;
+    for (int f = 0; f < SAMS_NFIELDS; ++f) ctx_.f[f] = nullptr;
+    for (int s = 0; s < NSCRATCH; ++s) ctx_.s[s] = nullptr;
+}
+
 int Solver::set_bc(int field, int dim, int edge, int kind, double value)
 {
     if (field < 0 || field >= SAMS_NFIELDS || dim < 0 || dim > 2 || edge < 0 || edge > 1 || kind < SAMS_BC_NONE ||

@@ -39,6 +39,12 @@ public:
 
     // Returns a sams_status; on failure err holds the reason.
     int init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device);
+    // Set up over memory the solver does not own (fields, scratch, axes and
+    // scalars already placed in ctx); allocates nothing and frees nothing.
+    int init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, const Ctx &ctx, int device,
+                      cudaStream_t stream);
+    // Forget borrowed memory (call before destroying a borrowed solver).
+    void release_borrowed();
     int set_bc(int field, int dim, int edge, int kind, double value);
     int set_stream(cudaStream_t s);
     int upload(int field, const double *src, cudaMemcpyKind kind);
