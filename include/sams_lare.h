@@ -116,6 +116,41 @@ int sams_lare_phase_times(sams_lare_solver *h, double ms[5]);
 /* Number of kernel launches one sams_lare_step(h, 1) issues. */
 int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches);
 
+/* ---- Batched solves ----------------------------------------------------
+ * Many independent LARE3D solves (any mix of sizes, parameters and boundary
+ * conditions) stepped together: each phase of the step is one persistent
+ * launch over a worklist of tiles drawn from every solve in the batch, and
+ * each solve keeps its own CFL timestep.  The reference runs one
+ * simulationData per runner (shared_data.h:60-226, runner.h:564-586); a
+ * batch replaces N runners stepping one after another. */
+typedef struct sams_lare_batch sams_lare_batch;
+
+int sams_lare_batch_create(int device, sams_lare_batch **out);
+int sams_lare_batch_destroy(sams_lare_batch *b);
+int sams_lare_batch_set_stream(sams_lare_batch *b, void *stream);
+/* Add a solve (allocates its device state); *id identifies it. */
+int sams_lare_batch_add(sams_lare_batch *b, const sams_lare_params *params,
+                        const sams_lare_bcs *bcs, int *id);
+/* Remove a solve and free its device memory. */
+int sams_lare_batch_remove(sams_lare_batch *b, int id);
+int sams_lare_batch_upload_field(sams_lare_batch *b, int id, int field, const double *host_box);
+int sams_lare_batch_download_field(sams_lare_batch *b, int id, int field, double *host_box);
+/* Advance every solve in the batch nsteps steps (asynchronous). */
+int sams_lare_batch_step(sams_lare_batch *b, int64_t nsteps);
+/* Same, replaying a CUDA graph of nsteps batched steps. */
+int sams_lare_batch_step_graph(sams_lare_batch *b, int64_t nsteps);
+int sams_lare_batch_synchronize(sams_lare_batch *b);
+/* dt, time and step count of one solve (any pointer may be NULL). */
+int sams_lare_batch_get_state(sams_lare_batch *b, int id, double *dt, double *time, int64_t *step);
+/* Tile shape: x planes per tile and resident blocks per SM of the
+ * persistent launches. */
+int sams_lare_batch_set_tuning(sams_lare_batch *b, int tile_planes, int blocks_per_sm);
+/* Time each candidate tile shape on the live batch for trial_steps steps
+ * and keep the fastest; the solves' states are restored afterwards. */
+int sams_lare_batch_autotune(sams_lare_batch *b, int trial_steps, int *tile_planes,
+                             int *blocks_per_sm, double *ms_per_step);
+int sams_lare_batch_device_bytes(sams_lare_batch *b, int64_t *bytes);
+
 /* No counterpart in the reference.  Advance nsteps timesteps of a solve whose
  * 13 fields live in the caller's own device memory, allocating nothing: for
  * callers that cannot call cudaMalloc while running (a host code whose device

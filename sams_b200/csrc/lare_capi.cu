@@ -188,3 +188,128 @@ int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched solves (include/sams_lare.h, "batch" section)
+// ---------------------------------------------------------------------------
+#include "lare_batch.cuh"
+
+struct sams_lare_batch {
+    sams::Batch b;
+};
+
+namespace {
+int bpass(sams_lare_batch *h, int rc)
+{
+    if (rc != SAMS_OK) g_last_error = h->b.err;
+    return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int sams_lare_batch_create(int device, sams_lare_batch **out)
+{
+    if (!out) return fail(SAMS_ERR_INVALID, "sams_lare_batch_create: null argument");
+    *out = nullptr;
+    sams_lare_batch *h = new (std::nothrow) sams_lare_batch();
+    if (!h) return fail(SAMS_ERR_NOMEM, "host allocation failed");
+    int rc = h->b.init(device);
+    if (rc != SAMS_OK) {
+        g_last_error = h->b.err;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return SAMS_OK;
+}
+
+int sams_lare_batch_destroy(sams_lare_batch *h)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    delete h;
+    return SAMS_OK;
+}
+
+int sams_lare_batch_set_stream(sams_lare_batch *h, void *stream)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.set_stream(static_cast<cudaStream_t>(stream)));
+}
+
+int sams_lare_batch_add(sams_lare_batch *h, const sams_lare_params *p, const sams_lare_bcs *bcs, int *id)
+{
+    if (!h || !p || !bcs || !id) return fail(SAMS_ERR_INVALID, "null argument");
+    return bpass(h, h->b.add(*p, *bcs, id));
+}
+
+int sams_lare_batch_remove(sams_lare_batch *h, int id)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.remove(id));
+}
+
+int sams_lare_batch_upload_field(sams_lare_batch *h, int id, int field, const double *host_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.upload(id, field, host_box, cudaMemcpyDefault));
+}
+
+int sams_lare_batch_download_field(sams_lare_batch *h, int id, int field, double *host_box)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.download(id, field, host_box, cudaMemcpyDefault));
+}
+
+int sams_lare_batch_step(sams_lare_batch *h, int64_t nsteps)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.step(nsteps));
+}
+
+int sams_lare_batch_step_graph(sams_lare_batch *h, int64_t nsteps)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.step_graph(nsteps));
+}
+
+int sams_lare_batch_synchronize(sams_lare_batch *h)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.sync());
+}
+
+int sams_lare_batch_get_state(sams_lare_batch *h, int id, double *dt, double *time, int64_t *step)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    sams::Scalars s;
+    int rc = h->b.scalars(id, s);
+    if (rc) return bpass(h, rc);
+    if (s.status) return fail(SAMS_ERR_NONFINITE, "the CFL timestep of this solve became non-finite");
+    if (dt) *dt = s.dt;
+    if (time) *time = s.time;
+    if (step) *step = s.step;
+    return SAMS_OK;
+}
+
+int sams_lare_batch_set_tuning(sams_lare_batch *h, int tile_planes, int blocks_per_sm)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.set_tuning(tile_planes, blocks_per_sm));
+}
+
+int sams_lare_batch_autotune(sams_lare_batch *h, int trial_steps, int *tile_planes, int *blocks_per_sm,
+                             double *ms_per_step)
+{
+    if (!h) return fail(SAMS_ERR_INVALID, "null batch");
+    return bpass(h, h->b.autotune(trial_steps, tile_planes, blocks_per_sm, ms_per_step));
+}
+
+int sams_lare_batch_device_bytes(sams_lare_batch *h, int64_t *bytes)
+{
+    if (!h || !bytes) return fail(SAMS_ERR_INVALID, "null argument");
+    *bytes = h->b.device_bytes();
+    return SAMS_OK;
+}
+
+}  // extern "C"

@@ -51,6 +51,7 @@ struct Axes {
 
 struct Phys {
     double gamma, mu0, visc1, visc2_norm, dt_multiplier, eta_bg, eta0, j_max;
+    int resistive;  // per-solve resistive flag (read by the batched launcher)
 };
 
 // Per-solve device scalars.

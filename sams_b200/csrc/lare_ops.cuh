@@ -90,6 +90,7 @@ __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int
 // Sound speed on cells; with resistive MHD also keeps p_e, which the
 // predictor needs from before the Ohmic heating (lagran.cpp:121, 606).
 struct CellPrep {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -116,6 +117,7 @@ struct CellPrep {
 
 // Node density and sound speed (8-cell volume-weighted averages).
 struct NodePrep {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
@@ -143,6 +145,7 @@ struct NodePrep {
 // Edge viscosities.  dt is the previous step's (the CFL reduction of this
 // step runs later, lagran.cpp:155-156).
 struct Alpha {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
@@ -185,6 +188,7 @@ struct Alpha {
 // cell's CFL candidate (p_visc is consumed here and never stored).
 // Returns the candidate (DBL_MAX outside the CFL range).
 struct Visc {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
@@ -287,6 +291,7 @@ struct Visc {
 // evaluated at the same point from the same B, so computed once), edge
 // electric fields and Ohmic heating rate.
 struct ResistRK {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -317,6 +322,7 @@ struct ResistRK {
 // heating; on the last sub-step also keeps the pre-update face B as b1,
 // which the predictor reads (resistive_effects' copy, lagran.cpp:482-484).
 struct ResistB {
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -361,6 +367,7 @@ struct ResistB {
 // Predictor, part 1: half-step cell volume and B (then scaled by cv1), and
 // the half-step pressures (lagran.cpp:598-614, 806-882).
 struct Pred1 {
+    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -452,6 +459,7 @@ struct Pred1 {
 // Predictor, part 2: pressure and J x B forces on nodes and the half-step
 // velocity (lagran.cpp:619-733, Cartesian).
 struct Pred2 {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -529,6 +537,7 @@ struct Pred2 {
 // Corrector, part 1: shock heating with the half-step velocities
 // (lagran.cpp:884-993, including its dy*dy factors at :987).
 struct Corr1 {
+    static constexpr int kMinBlocks = 2;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
@@ -569,6 +578,7 @@ struct Corr1 {
 // (lagran.cpp:754-798).  The corrector's cv1 is not kept: the x sweep
 // recomputes it over the whole range before any read.
 struct Corr2 {
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -615,6 +625,7 @@ struct Corr2 {
 // B to flux form (remap.cpp:46-50) when arg = 0, back to B with the
 // none_zero guard (remap.cpp:91-95) when arg = 1.
 struct BScale {
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
@@ -653,6 +664,7 @@ __device__ __forceinline__ long long dir_stride(const Geom &g, int dir)
 // adding zero does not change the sum.
 template <int DIR>
 struct SweepVol {
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -713,6 +725,7 @@ struct SweepVol {
 };
 
 struct SweepCvc {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
@@ -730,6 +743,7 @@ struct SweepCvc {
 // Both constrained-transport fluxes of a sweep.
 template <int DIR>
 struct SweepCT {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -778,6 +792,7 @@ struct SweepCT {
 // yremap.cpp:97-127, zremap.cpp:103-121), in the reference's order.
 template <int DIR>
 struct SweepCTUpd {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -841,6 +856,7 @@ __device__ __forceinline__ double face_area(const Ctx &c, int i, int j, int k)
 
 template <int DIR>
 struct SweepMass {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, DIR == 0 ? g.nx : g.nx + 1, 0, DIR == 1 ? g.ny : g.ny + 1, 0,
@@ -870,6 +886,7 @@ __device__ __forceinline__ bool in_sweep_range(int q, int n, int alo, int ahi_of
 // shift (xremap.cpp:121-221 and the y/z analogues).
 template <int DIR>
 struct SweepS6 {
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, DIR == 0 ? -2 : 0, DIR == 0 ? g.nx + 1 : g.nx, DIR == 1 ? -2 : 0,
@@ -926,6 +943,7 @@ struct SweepS6 {
 // Energy updates (1..n)^3 and the three momentum fluxes (times dm).
 template <int DIR>
 struct SweepS7 {
+    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, DIR == 0 ? -1 : 0, g.nx, DIR == 1 ? -1 : 0, g.ny, DIR == 2 ? -1 : 0, g.nz);
@@ -964,6 +982,7 @@ struct SweepS7 {
 // (xremap.cpp:226-261).
 template <int DIR>
 struct SweepS8 {
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);

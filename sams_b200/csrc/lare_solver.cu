@@ -27,7 +27,7 @@ constexpr int kThreads = 256;
 
 // One thread per (j, k) of a plane, blockIdx.y walks i.
 template <class Op>
-__global__ void __launch_bounds__(kThreads) k_op(Ctx c, int arg)
+__global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
 {
     int lo[3], hi[3];
     Op::bounds(c.g, arg, lo, hi);
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kThreads) k_op(Ctx c, int arg)
 // Visc with the CFL minimum: each block reduces its candidates and folds
 // them into Scalars::dtmin_bits.  Positive doubles order like their bit
 // patterns, so an integer atomicMin is an exact, order-free minimum.
-__global__ void __launch_bounds__(kThreads) k_visc(Ctx c)
+__global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
 {
     int lo[3], hi[3];
     ops::Visc::bounds(c.g, 0, lo, hi);
@@ -337,6 +337,7 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     ctx_.p.eta_bg = p.eta_background;
     ctx_.p.eta0 = p.eta0;
     ctx_.p.j_max = p.j_max;
+    ctx_.p.resistive = p.resistive_mhd ? 1 : 0;
 
     if ((rc = check(cudaMalloc(&sc_, sizeof(Scalars)), "cudaMalloc(scalars)"))) return rc;
     Scalars s0{};

@@ -239,3 +239,112 @@ class LARE3D:
 
     def set_stream(self, stream_ptr):
         _check(lib().sams_lare_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+
+def _bind_batch(L):
+    if getattr(L, "_batch_bound", False):
+        return
+    vp, i64 = ctypes.c_void_p, ctypes.c_int64
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.sams_lare_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.sams_lare_batch_destroy.argtypes = [vp]
+    L.sams_lare_batch_set_stream.argtypes = [vp, vp]
+    L.sams_lare_batch_add.argtypes = [vp, ctypes.POINTER(Params), ctypes.POINTER(Bcs), ip]
+    L.sams_lare_batch_remove.argtypes = [vp, ctypes.c_int]
+    L.sams_lare_batch_upload_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, _P]
+    L.sams_lare_batch_download_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, _P]
+    L.sams_lare_batch_step.argtypes = [vp, i64]
+    L.sams_lare_batch_step_graph.argtypes = [vp, i64]
+    L.sams_lare_batch_synchronize.argtypes = [vp]
+    L.sams_lare_batch_get_state.argtypes = [vp, ctypes.c_int, _P, _P, ctypes.POINTER(i64)]
+    L.sams_lare_batch_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.sams_lare_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, _P]
+    L.sams_lare_batch_device_bytes.argtypes = [vp, ctypes.POINTER(i64)]
+    L._batch_bound = True
+
+
+class Batch:
+    """Many independent LARE3D solves stepped together on one GPU (each
+    phase one persistent launch over all solves' tiles; each solve keeps its
+    own CFL timestep)."""
+
+    def __init__(self, device=0):
+        L = lib()
+        _bind_batch(L)
+        h = ctypes.c_void_p()
+        _check(L.sams_lare_batch_create(device, ctypes.byref(h)))
+        self._h = h
+        self.shapes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sams_lare_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, params, bcs, fields=None):
+        i = ctypes.c_int()
+        _check(lib().sams_lare_batch_add(self._h, ctypes.byref(params), ctypes.byref(bcs), ctypes.byref(i)))
+        self.shapes[i.value] = box_shape(params.nx, params.ny, params.nz)
+        if fields is not None:
+            for f, a in enumerate(fields):
+                self.upload(i.value, f, a)
+            self.synchronize()
+        return i.value
+
+    def remove(self, sid):
+        _check(lib().sams_lare_batch_remove(self._h, sid))
+        self.shapes.pop(sid, None)
+
+    def upload(self, sid, field, arr):
+        f = FIELD[field] if isinstance(field, str) else field
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self.shapes[sid]:
+            raise ValueError(f"expected box shape {self.shapes[sid]}, got {a.shape}")
+        self._keep = a  # the copy is asynchronous
+        _check(lib().sams_lare_batch_upload_field(self._h, sid, f, a.ctypes.data_as(_P)))
+        _check(lib().sams_lare_batch_synchronize(self._h))
+
+    def download(self, sid, field, out=None):
+        f = FIELD[field] if isinstance(field, str) else field
+        if out is None:
+            out = np.empty(self.shapes[sid])
+        _check(lib().sams_lare_batch_download_field(self._h, sid, f, out.ctypes.data_as(_P)))
+        return out
+
+    def step(self, n=1, graph=False):
+        if graph:
+            _check(lib().sams_lare_batch_step_graph(self._h, n))
+        else:
+            _check(lib().sams_lare_batch_step(self._h, n))
+
+    def synchronize(self):
+        _check(lib().sams_lare_batch_synchronize(self._h))
+
+    def state(self, sid):
+        dt, tm, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _check(lib().sams_lare_batch_get_state(self._h, sid, ctypes.byref(dt), ctypes.byref(tm), ctypes.byref(st)))
+        return dt.value, tm.value, st.value
+
+    def set_tuning(self, tile_planes, blocks_per_sm):
+        _check(lib().sams_lare_batch_set_tuning(self._h, tile_planes, blocks_per_sm))
+
+    def autotune(self, trial_steps=2):
+        t, b, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(lib().sams_lare_batch_autotune(self._h, trial_steps, ctypes.byref(t), ctypes.byref(b),
+                                              ctypes.byref(ms)))
+        return t.value, b.value, ms.value
+
+    @property
+    def device_bytes(self):
+        v = ctypes.c_int64()
+        _check(lib().sams_lare_batch_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def set_stream(self, stream_ptr):
+        _check(lib().sams_lare_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
