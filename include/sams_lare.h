@@ -151,6 +151,50 @@ int sams_lare_batch_autotune(sams_lare_batch *b, int trial_steps, int *tile_plan
                              int *blocks_per_sm, double *ms_per_step);
 int sams_lare_batch_device_bytes(sams_lare_batch *b, int64_t *bytes);
 
+/* ---- Serving: continuous batching under a device-memory budget ----------
+ * A scheduler thread keeps a batch of running solves resident on the GPU and
+ * advances them together one step at a time; queued requests are admitted in
+ * arrival order as soon as their device footprint fits the budget, and each
+ * finished solve's state is copied to the host and its memory freed.  The
+ * reference has no serving layer (one runner = one solve, runner.h:564-586). */
+typedef struct sams_lare_server sams_lare_server;
+
+enum sams_serve_status {
+    SAMS_SERVE_QUEUED = 0,
+    SAMS_SERVE_RUNNING = 1,
+    SAMS_SERVE_DONE = 2,
+    SAMS_SERVE_FAILED = 3
+};
+
+typedef struct sams_lare_serve_stats {
+    int64_t submitted, completed, failed, queued, running;
+    double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> result on host */
+    double cell_updates, wall_s, cell_updates_per_s;      /* since creation */
+    int64_t device_bytes_in_use;
+} sams_lare_serve_stats;
+
+int sams_lare_serve_create(int device, int64_t budget_bytes, sams_lare_server **out);
+/* Queue a solve of nsteps steps.  ic[f] are 13 host box buffers read when the
+ * solve is admitted (keep them valid until the status is RUNNING or later).
+ * out[q] receive the final rho, e_e, e_i, vx, vy, vz, bx, by, bz (box
+ * buffers, valid until DONE); with out == NULL the server keeps the result
+ * for sams_lare_serve_fetch.  Rejects a solve larger than the whole budget
+ * with SAMS_ERR_BUDGET. */
+int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *params,
+                           const sams_lare_bcs *bcs, const double *const ic[SAMS_NFIELDS],
+                           int64_t nsteps, double *const out[9], int64_t *ticket);
+/* Status (sams_serve_status) and latency so far / at completion. */
+int sams_lare_serve_poll(sams_lare_server *s, int64_t ticket, int *status, double *latency_s);
+/* Copy one of the nine kept result fields (index as for out[]). */
+int sams_lare_serve_fetch(sams_lare_server *s, int64_t ticket, int state_index, double *host_box);
+/* Forget a finished request (frees a kept result). */
+int sams_lare_serve_release(sams_lare_server *s, int64_t ticket);
+/* Wait until nothing is queued or running (SAMS_ERR_TIMEOUT otherwise). */
+int sams_lare_serve_drain(sams_lare_server *s, double timeout_s);
+int sams_lare_serve_get_stats(sams_lare_server *s, sams_lare_serve_stats *stats);
+/* Stop the scheduler and free everything. */
+int sams_lare_serve_destroy(sams_lare_server *s);
+
 /* No counterpart in the reference.  Advance nsteps timesteps of a solve whose
  * 13 fields live in the caller's own device memory, allocating nothing: for
  * callers that cannot call cudaMalloc while running (a host code whose device

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libsams_lare.so")
 
-CU_SOURCES = ["lare_solver.cu", "lare_batch.cu", "lare_capi.cu", "lare_noalloc.cu"]
+CU_SOURCES = ["lare_solver.cu", "lare_batch.cu", "lare_serve.cu", "lare_capi.cu", "lare_noalloc.cu"]
 C_SOURCES = ["lare_ic.c"]
 HEADERS = ["lare_device.cuh", "lare_ops.cuh", "lare_solver.cuh", "lare_batch.cuh"]
 
@@ -47,18 +47,19 @@ def build(verbose=False, force=False):
     deps += [os.path.join(ROOT, "include", h) for h in os.listdir(os.path.join(ROOT, "include")) if h.endswith(".h")]
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES:
         obj = os.path.join(LIBDIR, src + ".o")
-        cmd = [nvcc()] + NVCC_FLAGS + inc + ["-c", os.path.join(CSRC, src), "-o", obj]
-        _run(cmd, verbose)
+        cmds.append([nvcc()] + NVCC_FLAGS + inc + ["-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     for src in C_SOURCES:
         obj = os.path.join(LIBDIR, src + ".o")
-        cmd = ["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-fopenmp"] + inc + \
-              ["-c", os.path.join(CSRC, src), "-o", obj]
-        _run(cmd, verbose)
+        cmds.append(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-fopenmp"] + inc +
+                    ["-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(8, len(cmds))) as ex:
+        list(ex.map(lambda c: _run(c, verbose), cmds))
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + \
           ["-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"]
     _run(cmd, verbose)

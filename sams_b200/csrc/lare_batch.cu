@@ -67,13 +67,18 @@ __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
         const int ek = c.g.nz + 5, ej = c.g.ny + 5;
         const int p = tl.p0 + (int)threadIdx.x;
         double best = DBL_MAX;
+        bool bad = false;
         if (p < ej * ek) {
             const int j = -2 + p / ek, k = -2 + p % ek;
             if (j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
                 const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
-                for (int i = ia; i <= ib; ++i) best = dev::pmin(best, ops::Visc::run(c, 0, i, j, k));
+                for (int i = ia; i <= ib; ++i) {
+                    double cand = ops::Visc::run(c, 0, i, j, k, bad);
+                    best = dev::pmin(best, cand);
+                }
             }
         }
+        if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c.sc->status, 1);
         for (int off = 16; off > 0; off >>= 1) best = dev::pmin(best, __shfl_xor_sync(0xffffffffu, best, off));
         if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
         __syncthreads();
@@ -104,7 +109,7 @@ __global__ void kb_dt_finalize(const Ctx *__restrict__ ctxs, const int *__restri
         sc->dt_sub = dt / (double)nsub;
     }
     sc->dtmin_bits = (unsigned long long)__double_as_longlong(DBL_MAX);
-    if (!(dt > 0.0) || !(dt < DBL_MAX)) sc->status = 1;
+    if (!(m < DBL_MAX) || !(dt > 0.0) || !(dt < DBL_MAX)) sc->status = 1;
     sc->time += dt;
     sc->step += 1;
 }

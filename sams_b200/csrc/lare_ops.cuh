@@ -193,7 +193,10 @@ struct Visc {
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
     }
-    __device__ static double run(const Ctx &c, int, int i, int j, int k)
+    // nonfinite is set when a NaN or infinity shows up in this cell's viscous
+    // pressure, heating or CFL terms (the solve's state is no longer finite;
+    // the min itself would hide it, as LARE's min does).
+    __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
     {
         const Geom &g = c.g;
         const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
@@ -283,6 +286,8 @@ struct Visc {
         double dt2 = volume / pmax(pmax(pmax(avxm, avxp), dvx), 1.0e-10 * volume);
         double dt3 = volume / pmax(pmax(pmax(avym, avyp), dvy), 1.0e-10 * volume);
         double dt4 = volume / pmax(pmax(pmax(avzm, avzp), dvz), 1.0e-10 * volume);
+        const double chk = dt1 + dt2 + dt3 + dt4 + p_visc + vh;
+        if (!(fabs(chk) <= DBL_MAX)) nonfinite = true;
         return pmin(pmin(pmin(dt1, dt2), dt3), dt4);
     }
 };

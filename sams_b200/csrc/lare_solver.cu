@@ -51,14 +51,16 @@ __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long plane = (long long)(hi[1] - lo[1] + 1) * nk;
     double best = DBL_MAX;
+    bool bad = false;
     if (t < plane) {
         const int j = lo[1] + (int)(t / nk);
         const int k = lo[2] + (int)(t % nk);
         for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) {
-            double cand = ops::Visc::run(c, 0, i, j, k);
+            double cand = ops::Visc::run(c, 0, i, j, k, bad);
             best = dev::pmin(best, cand);
         }
     }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c.sc->status, 1);
     for (int off = 16; off > 0; off >>= 1) best = dev::pmin(best, __shfl_xor_sync(0xffffffffu, best, off));
     __shared__ double wmin[kThreads / 32];
     if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
@@ -87,7 +89,7 @@ __global__ void k_dt_finalize(Scalars *sc, double dt_multiplier, int resistive)
         sc->dt_sub = dt / (double)nsub;
     }
     sc->dtmin_bits = (unsigned long long)__double_as_longlong(DBL_MAX);
-    if (!(dt > 0.0) || !(dt < DBL_MAX)) sc->status = 1;
+    if (!(m < DBL_MAX) || !(dt > 0.0) || !(dt < DBL_MAX)) sc->status = 1;
     sc->time += dt;
     sc->step += 1;
 }

@@ -348,3 +348,91 @@ class Batch:
 
     def set_stream(self, stream_ptr):
         _check(lib().sams_lare_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("queued", ctypes.c_int64), ("running", ctypes.c_int64),
+                ("p50_latency_s", ctypes.c_double), ("p99_latency_s", ctypes.c_double),
+                ("mean_latency_s", ctypes.c_double), ("cell_updates", ctypes.c_double),
+                ("wall_s", ctypes.c_double), ("cell_updates_per_s", ctypes.c_double),
+                ("device_bytes_in_use", ctypes.c_int64)]
+
+
+SERVE_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+
+
+def _bind_serve(L):
+    if getattr(L, "_serve_bound", False):
+        return
+    vp, i64 = ctypes.c_void_p, ctypes.c_int64
+    L.sams_lare_serve_create.argtypes = [ctypes.c_int, i64, ctypes.POINTER(vp)]
+    L.sams_lare_serve_submit.argtypes = [vp, ctypes.POINTER(Params), ctypes.POINTER(Bcs), ctypes.POINTER(_P), i64,
+                                         ctypes.POINTER(_P), ctypes.POINTER(i64)]
+    L.sams_lare_serve_poll.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_int), _P]
+    L.sams_lare_serve_fetch.argtypes = [vp, i64, ctypes.c_int, _P]
+    L.sams_lare_serve_release.argtypes = [vp, i64]
+    L.sams_lare_serve_drain.argtypes = [vp, ctypes.c_double]
+    L.sams_lare_serve_get_stats.argtypes = [vp, ctypes.POINTER(ServeStats)]
+    L.sams_lare_serve_destroy.argtypes = [vp]
+    L._serve_bound = True
+
+
+class Server:
+    """Continuous-batching LARE3D server on one GPU (include/sams_lare.h,
+    serving section).  Submitted solves are admitted as device memory within
+    `budget_bytes` frees up, stepped together with every other running solve,
+    and their final state copied back when their step count is reached."""
+
+    def __init__(self, budget_bytes, device=0):
+        L = lib()
+        _bind_serve(L)
+        h = ctypes.c_void_p()
+        _check(L.sams_lare_serve_create(device, int(budget_bytes), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sams_lare_serve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, params, bcs, ic, nsteps, out=None):
+        ic = [np.ascontiguousarray(a, dtype=np.float64) for a in ic]
+        ip = (_P * NFIELDS)(*[a.ctypes.data_as(_P) for a in ic])
+        op = None
+        if out is not None:
+            op = (_P * 9)(*[a.ctypes.data_as(_P) for a in out])
+        t = ctypes.c_int64()
+        _check(lib().sams_lare_serve_submit(self._h, ctypes.byref(params), ctypes.byref(bcs), ip, int(nsteps),
+                                            op, ctypes.byref(t)))
+        self._keep[t.value] = (ic, out, box_shape(params.nx, params.ny, params.nz))
+        return t.value
+
+    def poll(self, ticket):
+        st, lat = ctypes.c_int(), ctypes.c_double()
+        _check(lib().sams_lare_serve_poll(self._h, ticket, ctypes.byref(st), ctypes.byref(lat)))
+        return SERVE_STATUS[st.value], lat.value
+
+    def fetch(self, ticket, index):
+        out = np.empty(self._keep[ticket][2])
+        _check(lib().sams_lare_serve_fetch(self._h, ticket, index, out.ctypes.data_as(_P)))
+        return out
+
+    def release(self, ticket):
+        _check(lib().sams_lare_serve_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+
+    def drain(self, timeout_s=600.0):
+        _check(lib().sams_lare_serve_drain(self._h, float(timeout_s)))
+
+    def stats(self):
+        s = ServeStats()
+        _check(lib().sams_lare_serve_get_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServeStats._fields_}

@@ -1,0 +1,76 @@
+"""Serving: continuous batching under a device-memory budget.  Solves that
+arrive while others run are admitted when memory frees up and stepped in
+the same batch; each result must equal the same solve run alone, bit for
+bit.  A solve that goes non-finite fails alone."""
+import time
+
+import numpy as np
+import pytest
+
+from sams_b200 import lare
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
+REQS = [("rf", (16, 16, 16), 12, 1), ("rf", (20, 16, 12), 9, 2), ("ot", (32, 24, 4), 15, 3),
+        ("harris", (24, 16, 8), 10, 4), ("rf", (24, 24, 24), 7, 5), ("ot", (48, 16, 6), 5, 6)]
+
+
+def _solo(case, n, steps, seed):
+    p, b = lare.case_setup(case, *n)
+    s = lare.LARE3D(p, b)
+    s.upload_all(lare.case_fields(case, p, seed=seed))
+    s.step(steps)
+    out = {f: s.download(f) for f in STATE}
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("budget_mb", [4096, 60])
+def test_served_results_equal_solo(budget_mb):
+    """budget 4 GB: everything runs concurrently; 60 MB: admissions wait for
+    earlier solves to finish (continuous batching under a tight budget)."""
+    srv = lare.Server(budget_mb << 20)
+    tickets = []
+    outs = []
+    for case, n, steps, seed in REQS:
+        p, b = lare.case_setup(case, *n)
+        out = [np.zeros(lare.box_shape(*n)) for _ in range(9)]
+        tickets.append(srv.submit(p, b, lare.case_fields(case, p, seed=seed), steps, out))
+        outs.append(out)
+        time.sleep(0.01)  # staggered arrivals
+    srv.drain(300)
+    st = srv.stats()
+    assert st["completed"] == len(REQS) and st["failed"] == 0
+    assert st["p99_latency_s"] >= st["p50_latency_s"] > 0
+    for t, out, (case, n, steps, seed) in zip(tickets, outs, REQS):
+        assert srv.poll(t)[0] == "done"
+        ref = _solo(case, n, steps, seed)
+        for q, f in enumerate(STATE):
+            sl = lare.field_slices(f, *n)
+            assert np.array_equal(out[q][sl], ref[f][sl]), f"{case}{n} {f}"
+    srv.close()
+
+
+def test_failed_solve_is_isolated_and_kept_results_fetchable():
+    srv = lare.Server(1 << 30)
+    p, b = lare.case_setup("rf", 12, 12, 12)
+    bad = lare.case_fields("rf", p, seed=1)
+    bad[0][:] = 0.0                       # zero density: the CFL timestep is not finite
+    tb = srv.submit(p, b, bad, 70)
+    good = srv.submit(p, b, lare.case_fields("rf", p, seed=2), 8)  # result kept by the server
+    srv.drain(300)
+    assert srv.poll(tb)[0] == "failed"
+    assert srv.poll(good)[0] == "done"
+    ref = _solo("rf", (12, 12, 12), 8, 2)
+    for q, f in enumerate(STATE):
+        sl = lare.field_slices(f, 12, 12, 12)
+        assert np.array_equal(srv.fetch(good, q)[sl], ref[f][sl]), f
+    srv.release(good)
+    srv.close()
+    tiny = lare.Server(1 << 20)           # 1 MB: a 16^3 solve can never fit
+    p16, b16 = lare.case_setup("rf", 16, 16, 16)
+    with pytest.raises(lare.LareError) as e:
+        tiny.submit(p16, b16, lare.case_fields("rf", p16), 1)
+    assert e.value.status == -7
+    tiny.close()
