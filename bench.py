@@ -46,11 +46,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sams", choices=["sams", "reference"])
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--edge", type=int, default=256, help="cube edge of the plain workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--serve-seconds", type=float, default=45.0)
+    ap.add_argument("--serve-max-cells", type=int, default=16 << 20)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -166,10 +170,27 @@ def cpu_reference(n, steps, threads=None):
     return secs, "port", threads
 
 
+def max_over_ranks(pg, ms, device):
+    """The slowest rank's time: replicas finish together only when the last
+    one does.  Every rank takes part (the same collective on every rank)."""
+    if pg is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, cells, steps, ms):
+    """Whole-job cell-updates/s of `world` independent replicas, each
+    advancing `cells` cells `steps` steps, in `ms` (max over ranks)."""
+    return world * cells * steps / (ms / 1e3)
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    n = args.n
+    n = args.edge
     total = args.warmup + args.steps
     secs, kind, threads = cpu_reference(n, total)
     timed = secs[args.warmup:]
@@ -193,7 +214,7 @@ def run_sams(args, world, rank, local, pg):
     from sams_b200 import lare
 
     torch.cuda.set_device(local)
-    n = args.n
+    n = args.edge
     cells = float(n) ** 3
     p, b = lare.case_setup("rf", n, n, n)
     fields = lare.case_fields("rf", p, seed=1 + rank)
@@ -221,15 +242,12 @@ def run_sams(args, world, rank, local, pg):
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
     if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
         pg.barrier()
     s.synchronize()
     ms_per_step = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3)
+    value = replica_throughput(world, cells, args.steps, ms)
     phases = s.phase_times()
     s.synchronize()
     s.close()
@@ -262,21 +280,21 @@ def run_sams(args, world, rank, local, pg):
             lare._check(L.sams_lare_download_field(h, f, ctypes_addr(o)))
         e1.record(stream)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if pg is not None:
-            t = torch.tensor([ems], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
         box_bytes = int(np.prod(lare.box_shape(n, n, n))) * 8
-        e2e = {"value": world * cells * args.steps / (ems / 1e3), "unit": UNIT,
+        e2e = {"value": replica_throughput(world, cells, args.steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": len(state) * box_bytes / args.steps,
                "d2h_bytes_per_step": (len(state) * box_bytes + 8 * args.steps) / args.steps,
                "what": "state upload from pinned host memory, K steps each reading dt back, state download"}
         s2.close()
 
+    # the batched and served workloads are single-GPU configurations
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and world == 1:
         batched = run_batched(args, local, stream)
+    served = None
+    if args.serve_seconds > 0 and world == 1:
+        served = run_served(args, local)
 
     if rank != 0:
         return
@@ -307,6 +325,7 @@ def run_sams(args, world, rank, local, pg):
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": launches * args.steps,
         "batched": batched,
+        "served": served,
         "phases_ms": dict(zip(["lagrangian", "corrector", "remap_x", "remap_y", "remap_z"], phases)),
     }
     print(json.dumps(line), flush=True)
@@ -374,6 +393,62 @@ def run_batched(args, local, stream):
             "plain_sequential": seq, "speedup_vs_plain_sequential": bat / seq,
             "ms_per_batched_step": bat_ms / K, "tile_planes": tile, "blocks_per_sm": bps,
             "device_bytes": dev_bytes}
+
+
+def run_served(args, local):
+    """Config 4: Poisson arrivals of random-field cube solves (edge drawn from
+    {32,64,96,128,192}, 100..2000 steps, resistive), admitted by an HBM budget
+    into one continuously batched server; reports p50/p99 latency (arrival to
+    result on the host) over the requests completed inside the window and the
+    aggregate cell-updates/s.  Initial states come from a pool of two seeded
+    states per edge length (generating a fresh 192^3 state per request on the
+    host would outrun the arrival rate)."""
+    import random
+    from sams_b200 import lare
+
+    rng = random.Random(7)
+    edges = [32, 64, 96, 128, 192]
+    pool = {}
+    for e in edges:
+        p, b = lare.case_setup("rf", e, e, e)
+        pool[e] = (p, b, [lare.case_fields("rf", p, seed=s) for s in (11, 12)])
+    srv = lare.Server(int(args.budget_gb * (1 << 30)), device=local, max_cells=args.serve_max_cells)
+    t0 = time.perf_counter()
+    submitted, open_tickets, offered = 0, [], 0.0
+    next_t = rng.expovariate(args.rate)
+    while True:
+        now = time.perf_counter() - t0
+        if now >= args.serve_seconds:
+            break
+        if now >= next_t:
+            e = rng.choice(edges)
+            steps = rng.randint(100, 2000)
+            p, b, ics = pool[e]
+            open_tickets.append(srv.submit(p, b, ics[rng.randrange(2)], steps))
+            offered += float(e) ** 3 * steps
+            submitted += 1
+            next_t += rng.expovariate(args.rate)
+        still = []
+        for t in open_tickets:   # free kept results as requests finish
+            st, _ = srv.poll(t)
+            if st in ("done", "failed"):
+                srv.release(t)
+            else:
+                still.append(t)
+        open_tickets = still
+        time.sleep(0.002)
+    stats = srv.stats()
+    srv.close()
+    return {"workload": "Poisson %g req/s, rf cubes edge U{32,64,96,128,192}, steps U[100,2000], "
+                        "eta=1e-4, %g GB HBM budget, %g s window" % (args.rate, args.budget_gb, args.serve_seconds),
+            "submitted": submitted, "completed": stats["completed"], "failed": stats["failed"],
+            "queued_at_end": stats["queued"], "running_at_end": stats["running"],
+            "p50_latency_s": stats["p50_latency_s"], "p99_latency_s": stats["p99_latency_s"],
+            "mean_latency_s": stats["mean_latency_s"], "value": stats["cell_updates_per_s"], "unit": UNIT,
+            "offered_cell_updates_per_s": offered / args.serve_seconds,
+            "admission": "arrival order; HBM budget %g GB; at most %d interior cells running at once"
+                         % (args.budget_gb, args.serve_max_cells),
+            "note": "offered load exceeds one B200's capacity, so latency includes growing queueing"}
 
 
 def ctypes_addr(t):

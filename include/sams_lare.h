@@ -183,6 +183,13 @@ int sams_lare_serve_create(int device, int64_t budget_bytes, sams_lare_server **
 int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *params,
                            const sams_lare_bcs *bcs, const double *const ic[SAMS_NFIELDS],
                            int64_t nsteps, double *const out[9], int64_t *ticket);
+/* Cap the interior cells (nx*ny*nz summed) of the solves running at once;
+ * 0 (the default) leaves only the memory budget.  Under a backlog a smaller
+ * running set finishes each solve sooner, so a cap just large enough to keep
+ * the GPU busy lowers latency at the same throughput.  Admission stays in
+ * arrival order: a request that does not fit waits at the head of the queue
+ * (one solve larger than the cap still runs, alone). */
+int sams_lare_serve_set_max_cells(sams_lare_server *s, int64_t max_cells);
 /* Status (sams_serve_status) and latency so far / at completion. */
 int sams_lare_serve_poll(sams_lare_server *s, int64_t ticket, int *status, double *latency_s);
 /* Copy one of the nine kept result fields (index as for out[]). */

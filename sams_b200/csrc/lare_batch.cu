@@ -127,7 +127,12 @@ __device__ __forceinline__ int locate(const long long *off, int n, long long g)
 __device__ __forceinline__ int fld_lb(int f, int d) { return field_half(f, d) ? -2 : -1; }
 
 // Composite periodic fill (see k_bc_periodic in lare_solver.cu) for every
-// live solve whose fields in `mask` are all-periodic.
+// live solve whose fields in `mask` are all-periodic.  The flat index walks
+// the ghost shell of each solve's whole box (-2..n+2 outside the interior
+// 1..n: x slabs, then y slabs inside x, then z slabs inside x and y); a
+// point is decomposed once and then copied for every field whose own range
+// holds it.  The set of points each field receives and their sources are
+// those of the per-field fill.
 __global__ void kb_bc_periodic(const Ctx *__restrict__ ctxs, const int *__restrict__ live,
                                const unsigned *__restrict__ pfields, const long long *__restrict__ off, int nlive,
                                long long total, unsigned mask, int resistive_only)
@@ -138,49 +143,42 @@ __global__ void kb_bc_periodic(const Ctx *__restrict__ ctxs, const int *__restri
         if ((mask & ~pfields[li]) != 0) continue;
         const Ctx &c = ctxs[live[li]];
         if (resistive_only && !c.p.resistive) continue;
-        const long long t0 = gi - off[li];
         const Geom &g = c.g;
-        const int n[3] = {g.nx, g.ny, g.nz};
+        const int n0 = g.nx, n1 = g.ny, n2 = g.nz;
+        const int E1 = n1 + 5, E2 = n2 + 5;
+        int t = (int)(gi - off[li]);
+        int q0, q1, q2;
+        const int A = 5 * E1 * E2, B = n0 * 5 * E2;
+        if (t < A) {
+            const int gx = t / (E1 * E2), r = t - gx * (E1 * E2);
+            q0 = gx < 3 ? gx - 2 : n0 + gx - 2;
+            q1 = r / E2 - 2;
+            q2 = r - (q1 + 2) * E2 - 2;
+        } else if ((t -= A) < B) {
+            const int i = t / (5 * E2), r = t - i * (5 * E2);
+            const int gy = r / E2;
+            q0 = 1 + i;
+            q1 = gy < 3 ? gy - 2 : n1 + gy - 2;
+            q2 = r - gy * E2 - 2;
+        } else {
+            t -= B;
+            const int i = t / (n1 * 5), r = t - i * (n1 * 5);
+            const int j = r / 5, gz = r - j * 5;
+            q0 = 1 + i;
+            q1 = 1 + j;
+            q2 = gz < 3 ? gz - 2 : n2 + gz - 2;
+        }
+        const int s0 = q0 <= 0 ? q0 + n0 : (q0 > n0 ? q0 - n0 : q0);
+        const int s1 = q1 <= 0 ? q1 + n1 : (q1 > n1 ? q1 - n1 : q1);
+        const int s2 = q2 <= 0 ? q2 + n2 : (q2 > n2 ? q2 - n2 : q2);
+        const long long dst = box_off(g, q0, q1, q2), src = box_off(g, s0, s1, s2);
         for (int f = 0; f < SAMS_NFIELDS; ++f) {
             if (!(mask & (1u << f))) continue;
-            int lb[3], ext[3], gh[3];
-            for (int d = 0; d < 3; ++d) {
-                lb[d] = fld_lb(f, d);
-                ext[d] = n[d] + 3 - lb[d];
-                gh[d] = ext[d] - n[d];
-            }
-            const long long A = (long long)gh[0] * ext[1] * ext[2];
-            const long long B = (long long)n[0] * gh[1] * ext[2];
-            const long long C = (long long)n[0] * n[1] * gh[2];
-            long long t = t0;
-            int q[3];
-            if (t < A) {
-                int gx = (int)(t / ((long long)ext[1] * ext[2]));
-                long long r = t % ((long long)ext[1] * ext[2]);
-                q[0] = gx < 1 - lb[0] ? lb[0] + gx : n[0] + 1 + (gx - (1 - lb[0]));
-                q[1] = lb[1] + (int)(r / ext[2]);
-                q[2] = lb[2] + (int)(r % ext[2]);
-            } else if ((t -= A) < B) {
-                int i = (int)(t / ((long long)gh[1] * ext[2]));
-                long long r = t % ((long long)gh[1] * ext[2]);
-                int gy = (int)(r / ext[2]);
-                q[0] = 1 + i;
-                q[1] = gy < 1 - lb[1] ? lb[1] + gy : n[1] + 1 + (gy - (1 - lb[1]));
-                q[2] = lb[2] + (int)(r % ext[2]);
-            } else if ((t -= B) < C) {
-                int i = (int)(t / ((long long)n[1] * gh[2]));
-                long long r = t % ((long long)n[1] * gh[2]);
-                int gz = (int)(r % gh[2]);
-                q[0] = 1 + i;
-                q[1] = 1 + (int)(r / gh[2]);
-                q[2] = gz < 1 - lb[2] ? lb[2] + gz : n[2] + 1 + (gz - (1 - lb[2]));
-            } else {
+            // centred dimensions start at -1
+            if ((q0 < -1 && !field_half(f, 0)) || (q1 < -1 && !field_half(f, 1)) || (q2 < -1 && !field_half(f, 2)))
                 continue;
-            }
-            int s[3];
-            for (int d = 0; d < 3; ++d) s[d] = q[d] <= 0 ? q[d] + n[d] : (q[d] >= n[d] + 1 ? q[d] - n[d] : q[d]);
             double *a = c.f[f];
-            a[box_off(g, q[0], q[1], q[2])] = a[box_off(g, s[0], s[1], s[2])];
+            a[dst] = a[src];
         }
     }
 }
@@ -353,6 +351,15 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
     if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
     if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) { err = "empty domain"; return SAMS_ERR_INVALID; }
+    {
+        // tile planes and ghost shells are indexed with 32-bit integers
+        const long long e1 = p.ny + 5, e2 = p.nz + 5;
+        const long long shell = 5 * e1 * e2 + p.nx * 5 * e2 + p.nx * p.ny * 5;
+        if (e1 * e2 > INT32_MAX || shell > INT32_MAX) {
+            err = "a batched solve's y-z plane or ghost shell exceeds 2^31 points";
+            return SAMS_ERR_UNSUPPORTED;
+        }
+    }
     int rc;
     if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
     BatchSlot s;

@@ -114,6 +114,14 @@ namespace dev {
 constexpr double NONE_ZERO = DBL_EPSILON;  // LARE simulationData::none_zero
 constexpr double SIXTH = 1.0 / 6.0;
 
+// An array that no thread of the running kernel writes.  Its loads take the
+// read-only (non-coherent) path, so the compiler may move them across the
+// kernel's stores to other arrays and keep more of them in flight.
+struct RO {
+    const double *p;
+    __device__ __forceinline__ double operator[](long long i) const { return __ldg(p + i); }
+};
+
 // portableWrapper min/max semantics (include/pp/utils.h:277-335).
 __device__ __forceinline__ double pmin(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double pmax(double a, double b) { return a > b ? a : b; }
@@ -232,8 +240,9 @@ __device__ __forceinline__ double mom_flux_dm(double v_advect, double dt, double
 
 // Caramana edge viscosity (lagran.cpp:56-93).  v[a] are the four points
 // along the edge direction, o1/o2 the edge ends.
-__device__ __forceinline__ double edge_viscosity(double dt, double visc1, double v2n, const double *vx,
-                                                 const double *vy, const double *vz, const double *rho_v,
+template <class A>
+__device__ __forceinline__ double edge_viscosity(double dt, double visc1, double v2n, const A &vx,
+                                                 const A &vy, const A &vz, const A &rho_v,
                                                  double dvdots, double dx, double dxm, double dxp,
                                                  double cs_edge, long long o0, long long o1, long long o2,
                                                  long long o3)

@@ -99,14 +99,14 @@ struct CellPrep {
     {
         const Geom &g = c.g;
         const long long o = LOFF(i, j, k);
-        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         double bx1 = 0.5 * (bx[o] + bx[o - g.sx]);
         double by1 = 0.5 * (by[o] + by[o - g.sy]);
         double bz1 = 0.5 * (bz[o] + bz[o - 1]);
         const double gm = c.p.gamma;
-        double rho = c.f[SAMS_F_RHO][o];
-        double pe = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ELECTRON][o];
-        double pi = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ION][o];
+        double rho = __ldg(c.f[SAMS_F_RHO] + o);
+        double pe = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
+        double pi = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double p = pe + pi;
         double rmin = pmax(rho, NONE_ZERO);
         double b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
@@ -125,7 +125,7 @@ struct NodePrep {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const double *rho = c.f[SAMS_F_RHO], *cs = c.s[S_CS];
+        const RO rho{c.f[SAMS_F_RHO]}, cs{c.s[S_CS]};
         const int ip = i + 1, jp = j + 1, kp = k + 1;
         double cv0 = cv_at(c, i, j, k), cv1 = cv_at(c, ip, j, k), cv2 = cv_at(c, i, jp, k), cv3 = cv_at(c, ip, jp, k);
         double cv4 = cv_at(c, i, j, kp), cv5 = cv_at(c, ip, j, kp), cv6 = cv_at(c, i, jp, kp), cv7 = cv_at(c, ip, jp, kp);
@@ -145,7 +145,7 @@ struct NodePrep {
 // Edge viscosities.  dt is the previous step's (the CFL reduction of this
 // step runs later, lagran.cpp:155-156).
 struct Alpha {
-    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
@@ -153,8 +153,8 @@ struct Alpha {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
-        const double *rho_v = c.s[S_RHOV], *cs_v = c.s[S_CSV];
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
+        const RO rho_v{c.s[S_RHOV]}, cs_v{c.s[S_CSV]};
         const double dt = c.sc->dt, visc1 = c.p.visc1, v2n = c.p.visc2_norm;
         const long long o = LOFF(i, j, k);
         if (i >= 0 && j >= 0) {  // alpha1: (0..nx+1, 0..ny+2, 0..nz+2)
@@ -188,7 +188,7 @@ struct Alpha {
 // cell's CFL candidate (p_visc is consumed here and never stored).
 // Returns the candidate (DBL_MAX outside the CFL range).
 struct Visc {
-    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
@@ -199,8 +199,8 @@ struct Visc {
     __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
     {
         const Geom &g = c.g;
-        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
-        const double *a1a = c.s[S_A1], *a2a = c.s[S_A2], *a3a = c.s[S_A3];
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
+        const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
         const long long SX = g.sx, SY = g.sy;
         const long long o = LOFF(i, j, k);
         const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
@@ -263,9 +263,10 @@ struct Visc {
         }
         // CFL candidate of cell (i, j, k) (lagran.cpp:388-438)
         const double gm = c.p.gamma;
-        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
-        double rho = c.f[SAMS_F_RHO][o];
-        double pressure = (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ELECTRON][o] + (gm - 1.0) * rho * c.f[SAMS_F_ENERGY_ION][o];
+        const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
+        double rho = __ldg(c.f[SAMS_F_RHO] + o);
+        double pressure = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o) +
+                          (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double rho0 = pmax(rho, NONE_ZERO);
         double cs2 = gm * pressure / rho0;
         double w1 = (bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o]) / c.p.mu0 / rho0;
@@ -296,7 +297,7 @@ struct Visc {
 // evaluated at the same point from the same B, so computed once), edge
 // electric fields and Ohmic heating rate.
 struct ResistRK {
-    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -304,7 +305,7 @@ struct ResistRK {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+        const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dxc = c.ax.dxc[i + 2], dyc = c.ax.dyc[j + 2], dzc = c.ax.dzc[k + 2];
         double jx1 = (bz[o + SY] - bz[o]) / dyc - (by[o + 1] - by[o]) / dzc;
@@ -337,7 +338,7 @@ struct ResistB {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
-        const double *fx = c.s[S_FLUXX], *fy = c.s[S_FLUXY], *fz = c.s[S_FLUXZ];
+        const RO fx{c.s[S_FLUXX]}, fy{c.s[S_FLUXY]}, fz{c.s[S_FLUXZ]};
         const double dt = c.sc->dt_sub;
         double bxo = bx[o], byo = by[o], bzo = bz[o];
         if (last) {
@@ -360,11 +361,11 @@ struct ResistB {
             bz[o] = bzo + (fy[o] - fy[o - SX] + fy[o - SY] - fy[o - SX - SY] - fx[o] + fx[o - SY] - fx[o - SX] + fx[o - SX - SY]) * dt / area;
         }
         if (inx1 && iny1 && inz1) {
-            const double *curlb = c.s[S_CURLB];
+            const RO curlb{c.s[S_CURLB]};
             double sum_curlb = curlb[o] + curlb[o - SX] + curlb[o - SY] + curlb[o - SX - SY] +
                                curlb[o - 1] + curlb[o - SX - 1] + curlb[o - SY - 1] + curlb[o - SX - SY - 1];
             double *ee = c.f[SAMS_F_ENERGY_ELECTRON];
-            ee[o] += sum_curlb * dt / (8.0 * c.f[SAMS_F_RHO][o]);
+            ee[o] += sum_curlb * dt / (8.0 * __ldg(c.f[SAMS_F_RHO] + o));
         }
     }
 };
@@ -372,7 +373,7 @@ struct ResistB {
 // Predictor, part 1: half-step cell volume and B (then scaled by cv1), and
 // the half-step pressures (lagran.cpp:598-614, 806-882).
 struct Pred1 {
-    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -381,7 +382,7 @@ struct Pred1 {
     {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const double dt = c.sc->dt;
         const double dxb0 = c.ax.dxb[i + 2], dxbm = c.ax.dxb[i + 1];
         const double dyb0 = c.ax.dyb[j + 2], dybm = c.ax.dyb[j + 1];
@@ -431,7 +432,7 @@ struct Pred1 {
             b1y = c.s[S_B1Y][o];
             b1z = c.s[S_B1Z][o];
         } else {
-            const double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
+            const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
             b1x = 0.5 * (bx[o] + bx[o - SX]);
             b1y = 0.5 * (by[o] + by[o - SY]);
             b1z = 0.5 * (bz[o] + bz[o - 1]);
@@ -449,13 +450,14 @@ struct Pred1 {
 
         if (i < 0 || i > g.nx + 1 || j < 0 || j > g.ny + 1 || k < 0 || k > g.nz + 1) return;
         const double gm = c.p.gamma;
-        double rho = c.f[SAMS_F_RHO][o], ee = c.f[SAMS_F_ENERGY_ELECTRON][o], ei = c.f[SAMS_F_ENERGY_ION][o];
+        double rho = __ldg(c.f[SAMS_F_RHO] + o), ee = __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
+        double ei = __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double pe = resistive ? c.s[S_PE][o] : (gm - 1.0) * rho * ee;
         double pi = (gm - 1.0) * rho * ei;
         double dvv = cv1 / vol - 1.0;
         double e1_e = ee - pe * dvv / rho;
         double e1_i = ei - pi * dvv / rho;
-        e1_i += c.s[S_VH][o] * dt / 2.0 / rho;
+        e1_i += __ldg(c.s[S_VH] + o) * dt / 2.0 / rho;
         c.s[S_PE][o] = e1_e * (gm - 1.0) * rho * vol / cv1;
         c.s[S_PI][o] = e1_i * (gm - 1.0) * rho * vol / cv1;
     }
@@ -473,8 +475,8 @@ struct Pred2 {
     {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const double *pe = c.s[S_PE], *pi = c.s[S_PI], *cv1 = c.s[S_CV1];
-        const double *bx1 = c.s[S_B1X], *by1 = c.s[S_B1Y], *bz1 = c.s[S_B1Z];
+        const RO pe{c.s[S_PE]}, pi{c.s[S_PI]}, cv1{c.s[S_CV1]};
+        const RO bx1{c.s[S_B1X]}, by1{c.s[S_B1Y]}, bz1{c.s[S_B1Z]};
         const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
         const double dhy = dy, dhz = dz;
         const long long q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
@@ -532,10 +534,10 @@ struct Pred2 {
         c.s[S_FY][o] = fy;
         c.s[S_FZ][o] = fz;
         const double dt = c.sc->dt;
-        const double rho_v = c.s[S_RHOV][o];
-        c.f[SAMS_F_VX1][o] = c.f[SAMS_F_VX][o] + dt / 2.0 * (c.s[S_FXV][o] + fx) / rho_v;
-        c.f[SAMS_F_VY1][o] = c.f[SAMS_F_VY][o] + dt / 2.0 * (c.s[S_FYV][o] + fy) / rho_v;
-        c.f[SAMS_F_VZ1][o] = c.f[SAMS_F_VZ][o] + dt / 2.0 * (c.s[S_FZV][o] + fz) / rho_v;
+        const double rho_v = __ldg(c.s[S_RHOV] + o);
+        c.f[SAMS_F_VX1][o] = __ldg(c.f[SAMS_F_VX] + o) + dt / 2.0 * (__ldg(c.s[S_FXV] + o) + fx) / rho_v;
+        c.f[SAMS_F_VY1][o] = __ldg(c.f[SAMS_F_VY] + o) + dt / 2.0 * (__ldg(c.s[S_FYV] + o) + fy) / rho_v;
+        c.f[SAMS_F_VZ1][o] = __ldg(c.f[SAMS_F_VZ] + o) + dt / 2.0 * (__ldg(c.s[S_FZV] + o) + fz) / rho_v;
     }
 };
 
@@ -551,9 +553,9 @@ struct Corr1 {
     {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
-        const double *vx1 = c.f[SAMS_F_VX1], *vy1 = c.f[SAMS_F_VY1], *vz1 = c.f[SAMS_F_VZ1];
-        const double *a1a = c.s[S_A1], *a2a = c.s[S_A2], *a3a = c.s[S_A3];
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
+        const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
+        const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
 #define DD(a, b) (1 * ((vx[a] - vx[b]) * (vx1[a] - vx1[b]) + (vy[a] - vy[b]) * (vy1[a] - vy1[b]) + \
                        (vz[a] - vz[b]) * (vz1[a] - vz1[b])))
         const long long mm0 = o - SX - SY, m00 = o - SX, om0 = o - SY;
@@ -594,14 +596,14 @@ struct Corr2 {
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
         {
-            const double rho_v = c.s[S_RHOV][o];
+            const double rho_v = __ldg(c.s[S_RHOV] + o);
             double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
-            vx[o] += dt * (c.s[S_FXV][o] + c.s[S_FX][o]) / rho_v;
-            vy[o] += dt * (c.s[S_FYV][o] + c.s[S_FY][o]) / rho_v;
-            vz[o] += dt * (c.s[S_FZV][o] + c.s[S_FZ][o]) / rho_v;
+            vx[o] += dt * (__ldg(c.s[S_FXV] + o) + __ldg(c.s[S_FX] + o)) / rho_v;
+            vy[o] += dt * (__ldg(c.s[S_FYV] + o) + __ldg(c.s[S_FY] + o)) / rho_v;
+            vz[o] += dt * (__ldg(c.s[S_FZV] + o) + __ldg(c.s[S_FZ] + o)) / rho_v;
         }
         if (i < 1 || j < 1 || k < 1) return;
-        const double *vx1 = c.f[SAMS_F_VX1], *vy1 = c.f[SAMS_F_VY1], *vz1 = c.f[SAMS_F_VZ1];
+        const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
         const long long a = o, am = o - SX, bm = o - SY, cm = o - 1;
         double vxb = 0.25 * (vx1[a] + vx1[bm] + vx1[cm] + vx1[bm - 1]);
         double vxbm = 0.25 * (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]);
@@ -617,8 +619,8 @@ struct Corr2 {
         double dv = (dvxdx + dvydy + dvzdz) * dt;
         double *rho = c.f[SAMS_F_RHO], *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
         double r = rho[o];
-        ee[o] -= dv * c.s[S_PE][o] / r;
-        ei[o] += (dt * c.s[S_VH][o] - dv * c.s[S_PI][o]) / r;
+        ee[o] -= dv * __ldg(c.s[S_PE] + o) / r;
+        ei[o] += (dt * __ldg(c.s[S_VH] + o) - dv * __ldg(c.s[S_PI] + o)) / r;
         rho[o] = r / (1.0 + dv);
     }
 };
@@ -684,19 +686,19 @@ struct SweepVol {
         const long long am = o - SX, bm = o - SY, cm = o - 1;
         double tx = 0.0, ty = 0.0, tz = 0.0, vxb = 0.0, vxbm = 0.0, vyb = 0.0, vybm = 0.0, vzb = 0.0, vzbm = 0.0;
         if (DIR == 0) {
-            const double *vx1 = c.f[SAMS_F_VX1];
+            const RO vx1{c.f[SAMS_F_VX1]};
             vxb = (vx1[o] + vx1[bm] + vx1[cm] + vx1[bm - 1]) * 0.25;
             vxbm = (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]) * 0.25;
             tx = vxb * (dyb0 * dzb0) - vxbm * (dyb0 * dzb0);
         }
         if (DIR <= 1) {
-            const double *vy1 = c.f[SAMS_F_VY1];
+            const RO vy1{c.f[SAMS_F_VY1]};
             vyb = (vy1[o] + vy1[am] + vy1[cm] + vy1[am - 1]) * 0.25;
             vybm = (vy1[bm] + vy1[bm - SX] + vy1[bm - 1] + vy1[bm - SX - 1]) * 0.25;
             ty = vyb * (dxb0 * dzb0) - vybm * (dxb0 * dzb0);
         }
         {
-            const double *vz1 = c.f[SAMS_F_VZ1];
+            const RO vz1{c.f[SAMS_F_VZ1]};
             vzb = (vz1[o] + vz1[am] + vz1[bm] + vz1[am - SY]) * 0.25;
             vzbm = (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]) * 0.25;
             tz = vzb * (dxb0 * dyb0) - vzbm * (dxb0 * dyb0);
@@ -724,7 +726,7 @@ struct SweepVol {
         c.s[S_R_CV2][o] = cv2;
         c.s[S_R_CV1][o] = vol * (1.0 + dv);
         c.s[S_R_DB1][o] = db1;
-        c.s[S_R_RHO1][o] = c.f[SAMS_F_RHO][o];
+        c.s[S_R_RHO1][o] = __ldg(c.f[SAMS_F_RHO] + o);
         c.f[SAMS_F_DM][o] = 0.0;
     }
 };
@@ -739,7 +741,7 @@ struct SweepCvc {
     {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const double *cv1 = c.s[S_R_CV1];
+        const RO cv1{c.s[S_R_CV1]};
         c.s[S_R_CVC1][o] = 0.125 * (cv1[o] + cv1[o + SX] + cv1[o + SY] + cv1[o + SX + SY] +
                                     cv1[o + 1] + cv1[o + SX + 1] + cv1[o + SY + 1] + cv1[o + SX + SY + 1]);
     }
@@ -759,20 +761,20 @@ struct SweepCT {
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const long long d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
-        const double *db1 = c.s[S_R_DB1], *cvc1 = c.s[S_R_CVC1], *cv1 = c.s[S_R_CV1];
-        const double *v1 = c.f[SAMS_F_VX1 + DIR];
+        const RO db1{c.s[S_R_DB1]}, cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
+        const RO v1{c.f[SAMS_F_VX1 + DIR]};
         // transverse offsets of the two db1 samples averaged for each flux
         long long t1, t2, va1, va2;
-        const double *b1, *b2;
+        RO b1, b2;
         if (DIR == 0) {        // vx_by (avg +y, v avg -z), vx_bz (avg +z, v avg -y)
-            t1 = SY; va1 = -1; b1 = c.f[SAMS_F_BY];
-            t2 = 1;  va2 = -SY; b2 = c.f[SAMS_F_BZ];
+            t1 = SY; va1 = -1; b1.p = c.f[SAMS_F_BY];
+            t2 = 1;  va2 = -SY; b2.p = c.f[SAMS_F_BZ];
         } else if (DIR == 1) { // vy_bx (avg +x, v avg -z), vy_bz (avg +z, v avg -x)
-            t1 = SX; va1 = -1; b1 = c.f[SAMS_F_BX];
-            t2 = 1;  va2 = -SX; b2 = c.f[SAMS_F_BZ];
+            t1 = SX; va1 = -1; b1.p = c.f[SAMS_F_BX];
+            t2 = 1;  va2 = -SX; b2.p = c.f[SAMS_F_BZ];
         } else {               // vz_bx (avg +x, v avg -y), vz_by (avg +y, v avg -x)
-            t1 = SX; va1 = -SY; b1 = c.f[SAMS_F_BX];
-            t2 = SY; va2 = -SX; b2 = c.f[SAMS_F_BY];
+            t1 = SX; va1 = -SY; b1.p = c.f[SAMS_F_BX];
+            t2 = SY; va2 = -SX; b2.p = c.f[SAMS_F_BY];
         }
         const double dci = cvc1[o], dcm = cvc1[o - d], dcp = cvc1[o + d], cvi = cv1[o], cvp = cv1[o + d];
         {
@@ -806,7 +808,7 @@ struct SweepCTUpd {
     {
         const Geom &g = c.g;
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const double *f1 = c.s[S_R_CT1], *f2 = c.s[S_R_CT2];
+        const RO f1{c.s[S_R_CT1]}, f2{c.s[S_R_CT2]};
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
         const bool xb = i >= 0, xc = i >= 1, yb = j >= 0, yc = j >= 1, zb = k >= 0, zc = k >= 1;
         if (DIR == 0) {
@@ -842,13 +844,13 @@ __device__ __forceinline__ double face_velocity(const Ctx &c, long long o)
     const Geom &g = c.g;
     const long long SX = g.sx, SY = g.sy;
     if (DIR == 0) {
-        const double *v = c.f[SAMS_F_VX1];
+        const RO v{c.f[SAMS_F_VX1]};
         return (v[o] + v[o - SY] + v[o - 1] + v[o - SY - 1]) * 0.25;
     } else if (DIR == 1) {
-        const double *v = c.f[SAMS_F_VY1];
+        const RO v{c.f[SAMS_F_VY1]};
         return (v[o - SX] + v[o] + v[o - SX - 1] + v[o - 1]) * 0.25;
     } else {
-        const double *v = c.f[SAMS_F_VZ1];
+        const RO v{c.f[SAMS_F_VZ1]};
         return (v[o - SX] + v[o] + v[o - SX - SY] + v[o - SY]) * 0.25;
     }
 }
@@ -872,7 +874,7 @@ struct SweepMass {
         const Geom &g = c.g;
         const long long o = LOFF(i, j, k);
         const long long d = dir_stride(g, DIR);
-        const double *rho = c.f[SAMS_F_RHO], *cvc1 = c.s[S_R_CVC1], *cv1 = c.s[S_R_CV1];
+        const RO rho{c.f[SAMS_F_RHO]}, cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
         double v = face_velocity<DIR>(c, o);
         c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
                                       rho[o + 2 * d], cvc1[o], cvc1[o - d], cvc1[o + d], cv1[o], cv1[o + d]);
@@ -903,8 +905,8 @@ struct SweepS6 {
         const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const long long d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
-        const double *rho1 = c.s[S_R_RHO1], *cv1 = c.s[S_R_CV1], *cv2 = c.s[S_R_CV2], *cvc1 = c.s[S_R_CVC1];
-        const double *dm = c.f[SAMS_F_DM];
+        const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
+        const RO dm{c.f[SAMS_F_DM]};
         const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
         const int qd = DIR == 0 ? i : (DIR == 1 ? j : k);
         const bool all0n = i >= 0 && i <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
@@ -915,7 +917,7 @@ struct SweepS6 {
         if (all0n) {
             double v = face_velocity<DIR>(c, o);
             double area = face_area<DIR>(c, i, j, k);
-            const double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+            const RO ee{c.f[SAMS_F_ENERGY_ELECTRON]}, ei{c.f[SAMS_F_ENERGY_ION]};
             c.s[S_R_FE1][o] = energy_flux(v, dt, area, ee[o - d], ee[o], ee[o + d], ee[o + 2 * d], cvc1[o], cvc1[o - d],
                                           cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]);
             c.s[S_R_FE2][o] = energy_flux(v, dt, area, ei[o - d], ei[o], ei[o + d], ei[o + 2 * d], cvc1[o], cvc1[o - d],
@@ -939,7 +941,7 @@ struct SweepS6 {
         }
         // sweep-direction v1 moved to the face centre: -2..n+1 along, 0..n across
         {
-            const double *v1 = c.f[SAMS_F_VX1 + DIR];
+            const RO v1{c.f[SAMS_F_VX1 + DIR]};
             c.s[S_R_V1S][o] = (v1[o] + v1[o + d]) * 0.5;
         }
     }
@@ -959,21 +961,21 @@ struct SweepS7 {
         const long long o = LOFF(i, j, k);
         const long long d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
-        const double *rho1 = c.s[S_R_RHO1], *cv1 = c.s[S_R_CV1], *cv2 = c.s[S_R_CV2], *cvc1 = c.s[S_R_CVC1];
+        const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
         if (i >= 1 && j >= 1 && k >= 1) {
-            const double *f1 = c.s[S_R_FE1], *f2 = c.s[S_R_FE2];
+            const RO f1{c.s[S_R_FE1]}, f2{c.s[S_R_FE2]};
             double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
-            double den = cv2[o] * c.f[SAMS_F_RHO][o];
+            double den = cv2[o] * __ldg(c.f[SAMS_F_RHO] + o);
             ee[o] = (ee[o] * cv1[o] * rho1[o] + f1[o - d] - f1[o]) / den;
             ei[o] = (ei[o] * cv1[o] * rho1[o] + f2[o - d] - f2[o]) / den;
         }
-        const double *v1s = c.s[S_R_V1S], *rv = c.s[S_R_RVN], *dmn = c.s[S_R_DMN];
+        const RO v1s{c.s[S_R_V1S]}, rv{c.s[S_R_RVN]}, dmn{c.s[S_R_DMN]};
         // x sweep uses dxac; the y and z sweeps both use dyac (zremap.cpp:475)
         double area = DIR == 0 ? dxac_at(c, i, j, k) : dyac_at(c, i, j, k);
         const double v = v1s[o], dmv = dmn[o];
         const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
         const double rvi = rv[o], rvp = rv[o + d];
-        const double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
+        const RO ux{c.f[SAMS_F_VX]}, uy{c.f[SAMS_F_VY]}, uz{c.f[SAMS_F_VZ]};
         c.s[S_R_FM1][o] = mom_flux_dm<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
                                                 cvi, cvp, rvi, rvp, dmv);
         c.s[S_R_FM2][o] = mom_flux_dm<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
@@ -997,12 +999,12 @@ struct SweepS8 {
         const Geom &g = c.g;
         const long long o = LOFF(i, j, k);
         const long long d = dir_stride(g, DIR);
-        const double *rv = c.s[S_R_RVN], *cvc1 = c.s[S_R_CVC1], *cv2n = c.s[S_R_CV2N], *dmn = c.s[S_R_DMN];
+        const RO rv{c.s[S_R_RVN]}, cvc1{c.s[S_R_CVC1]}, cv2n{c.s[S_R_CV2N]}, dmn{c.s[S_R_DMN]};
         const double rvo = rv[o], cvco = cvc1[o], cv2o = cv2n[o];
         const double rho_v1 = (rvo * cvco + dmn[o - d] - dmn[o]) / cv2o;
         const double den = cv2o * rho_v1;
         double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
-        const double *f1 = c.s[S_R_FM1], *f2 = c.s[S_R_FM2], *f3 = c.s[S_R_FM3];
+        const RO f1{c.s[S_R_FM1]}, f2{c.s[S_R_FM2]}, f3{c.s[S_R_FM3]};
         ux[o] = (rvo * ux[o] * cvco + f1[o - d] - f1[o]) / den;
         uy[o] = (rvo * uy[o] * cvco + f2[o - d] - f2[o]) / den;
         uz[o] = (rvo * uz[o] * cvco + f3[o - d] - f3[o]) / den;

@@ -4,7 +4,8 @@
 // a step count) arrive at any time.  A scheduler thread owns one Batch and
 // loops:
 //   1. admit queued requests in arrival order while their device footprint
-//      fits the budget (allocate, upload the initial state);
+//      fits the budget and, when a cap is set, the interior cells of the
+//      running solves stay under it (allocate, upload the initial state);
 //   2. advance every running solve together by one batched step (one graph
 //      launch; the graph is re-recorded when the running set changes);
 //   3. retire solves that reached their step count: copy the state to the
@@ -42,6 +43,7 @@ struct Request {
     std::vector<std::vector<double>> staged;  // results kept by the server when out == NULL
     int64_t nsteps = 0;
     int64_t done = 0;
+    long long cells = 0;
     int slot = -1;
     int status = SAMS_SERVE_QUEUED;
     long long bytes = 0;
@@ -57,6 +59,8 @@ struct sams_lare_server {
     sams::Batch batch;
     long long budget = 0;
     long long in_use = 0;
+    long long max_cells = 0;       // cap on running interior cells (0 = none)
+    long long cells_in_use = 0;
     std::mutex mu;
     std::condition_variable cv;
     std::thread worker;
@@ -82,6 +86,9 @@ bool sams_lare_server::admit_locked()
     while (!queue.empty()) {
         Request *r = queue.front();
         if (in_use + r->bytes > budget && !running.empty()) break;  // wait for memory
+        // wait for work to drain: a smaller running set finishes each solve
+        // sooner once the set already keeps the GPU busy
+        if (max_cells > 0 && cells_in_use + r->cells > max_cells && !running.empty()) break;
         if (in_use + r->bytes > budget && running.empty() && r->bytes > budget) {
             // can never fit
             queue.pop_front();
@@ -108,6 +115,7 @@ bool sams_lare_server::admit_locked()
         r->status = SAMS_SERVE_RUNNING;
         r->t_admit = Clock::now();
         in_use += r->bytes;
+        cells_in_use += r->cells;
         running.push_back(r);
         any = true;
     }
@@ -128,9 +136,10 @@ void sams_lare_server::retire(Request *r, bool ok)
         }
     }
     batch.remove(r->slot);
-    in_use -= r->bytes;
     r->t_done = Clock::now();
     std::lock_guard<std::mutex> lk(mu);
+    in_use -= r->bytes;
+    cells_in_use -= r->cells;
     r->status = ok ? SAMS_SERVE_DONE : SAMS_SERVE_FAILED;
     if (ok) {
         ++completed;
@@ -158,6 +167,7 @@ void sams_lare_server::loop()
             for (Request *r : running) {
                 batch.remove(r->slot);
                 in_use -= r->bytes;
+                cells_in_use -= r->cells;
                 r->status = SAMS_SERVE_FAILED;
                 r->t_done = Clock::now();
                 ++failed;
@@ -244,6 +254,7 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
     for (int q = 0; q < 9; ++q) r->out[q] = out ? out[q] : nullptr;
     r->nsteps = nsteps;
     r->bytes = sams::Batch::bytes_for(*p);
+    r->cells = (long long)(p->nx * p->ny * p->nz);
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     if (r->bytes > s->budget) {
@@ -254,6 +265,18 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
     *ticket = r->id;
     s->queue.push_back(r.get());
     s->all.emplace(r->id, std::move(r));
+    s->cv.notify_all();
+    return SAMS_OK;
+}
+
+int sams_lare_serve_set_max_cells(sams_lare_server *s, int64_t max_cells)
+{
+    if (!s || max_cells < 0) {
+        sams_capi_set_last_error("sams_lare_serve_set_max_cells: null server or negative cap");
+        return SAMS_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->max_cells = (long long)max_cells;
     s->cv.notify_all();
     return SAMS_OK;
 }

@@ -369,6 +369,7 @@ def _bind_serve(L):
     L.sams_lare_serve_create.argtypes = [ctypes.c_int, i64, ctypes.POINTER(vp)]
     L.sams_lare_serve_submit.argtypes = [vp, ctypes.POINTER(Params), ctypes.POINTER(Bcs), ctypes.POINTER(_P), i64,
                                          ctypes.POINTER(_P), ctypes.POINTER(i64)]
+    L.sams_lare_serve_set_max_cells.argtypes = [vp, i64]
     L.sams_lare_serve_poll.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_int), _P]
     L.sams_lare_serve_fetch.argtypes = [vp, i64, ctypes.c_int, _P]
     L.sams_lare_serve_release.argtypes = [vp, i64]
@@ -384,13 +385,19 @@ class Server:
     `budget_bytes` frees up, stepped together with every other running solve,
     and their final state copied back when their step count is reached."""
 
-    def __init__(self, budget_bytes, device=0):
+    def __init__(self, budget_bytes, device=0, max_cells=0):
         L = lib()
         _bind_serve(L)
         h = ctypes.c_void_p()
         _check(L.sams_lare_serve_create(device, int(budget_bytes), ctypes.byref(h)))
         self._h = h
         self._keep = {}
+        if max_cells:
+            self.set_max_cells(max_cells)
+
+    def set_max_cells(self, max_cells):
+        """Cap the interior cells of the solves running at once (0 = none)."""
+        _check(lib().sams_lare_serve_set_max_cells(self._h, int(max_cells)))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -26,11 +26,13 @@ def _solo(case, n, steps, seed):
     return out
 
 
-@pytest.mark.parametrize("budget_mb", [4096, 60])
-def test_served_results_equal_solo(budget_mb):
+@pytest.mark.parametrize("budget_mb,max_cells", [(4096, 0), (60, 0), (4096, 9000)])
+def test_served_results_equal_solo(budget_mb, max_cells):
     """budget 4 GB: everything runs concurrently; 60 MB: admissions wait for
-    earlier solves to finish (continuous batching under a tight budget)."""
-    srv = lare.Server(budget_mb << 20)
+    earlier solves to finish (continuous batching under a tight budget);
+    a 9000-cell cap: at most two of these solves run at once, in arrival
+    order (the 13824-cell one runs alone)."""
+    srv = lare.Server(budget_mb << 20, max_cells=max_cells)
     tickets = []
     outs = []
     for case, n, steps, seed in REQS:
