@@ -272,13 +272,13 @@ Geom batch_geom(const sams_lare_params &p)
     g.nz = (int)p.nz;
     if (p.nz >= 32) {  // long rows: pad to 8 doubles with interior k = 1 on a 32-byte boundary
         g.zoff = 3;
-        g.sy = ((p.nz + 6) + 7) / 8 * 8;
+        g.sy = (int)(((p.nz + 6) + 7) / 8 * 8);
     } else {            // short rows (e.g. nz = 4): dense
         g.zoff = 2;
-        g.sy = p.nz + 5;
+        g.sy = (int)(p.nz + 5);
     }
-    g.sx = (p.ny + 5) * g.sy;
-    g.nelem = (p.nx + 5) * g.sx;
+    g.sx = (int)((p.ny + 5) * g.sy);
+    g.nelem = (p.nx + 5) * (long long)g.sx;
     return g;
 }
 
@@ -355,8 +355,9 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
         // tile planes and ghost shells are indexed with 32-bit integers
         const long long e1 = p.ny + 5, e2 = p.nz + 5;
         const long long shell = 5 * e1 * e2 + p.nx * 5 * e2 + p.nx * p.ny * 5;
-        if (e1 * e2 > INT32_MAX || shell > INT32_MAX) {
-            err = "a batched solve's y-z plane or ghost shell exceeds 2^31 points";
+        const long long rows = (p.nz >= 32 ? ((p.nz + 6) + 7) / 8 * 8 : e2) * e1 * (p.nx + 5);
+        if (rows > INT32_MAX || shell > INT32_MAX) {
+            err = "one array or the ghost shell of this solve exceeds 2^31 points";
             return SAMS_ERR_UNSUPPORTED;
         }
     }

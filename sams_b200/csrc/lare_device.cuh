@@ -22,15 +22,17 @@ namespace sams {
 
 struct Geom {
     int nx, ny, nz;
-    long long sx, sy;  // element strides of i and j (k stride is 1)
+    int sx, sy;        // element strides of i and j (k stride is 1)
     int zoff;          // k + zoff is the position of index k in its row
     long long nelem;   // doubles per field allocation
 };
 
 // Host/device helpers for the box geometry.
-__host__ __device__ inline long long box_off(const Geom &g, int i, int j, int k)
+// Offsets are 32-bit: the 32 arrays of a solve must fit one GPU, so a single
+// array holds far fewer than 2^31 elements (checked when a solve is set up).
+__host__ __device__ inline int box_off(const Geom &g, int i, int j, int k)
 {
-    return (long long)(i + 2) * g.sx + (long long)(j + 2) * g.sy + (long long)(k + g.zoff);
+    return (i + 2) * g.sx + (j + 2) * g.sy + (k + g.zoff);
 }
 
 // Staggering of a field in one dimension (1 = half cell), the device-side
@@ -119,7 +121,7 @@ constexpr double SIXTH = 1.0 / 6.0;
 // kernel's stores to other arrays and keep more of them in flight.
 struct RO {
     const double *p;
-    __device__ __forceinline__ double operator[](long long i) const { return __ldg(p + i); }
+    __device__ __forceinline__ double operator[](int i) const { return __ldg(p + i); }
 };
 
 // portableWrapper min/max semantics (include/pp/utils.h:277-335).
@@ -244,8 +246,7 @@ template <class A>
 __device__ __forceinline__ double edge_viscosity(double dt, double visc1, double v2n, const A &vx,
                                                  const A &vy, const A &vz, const A &rho_v,
                                                  double dvdots, double dx, double dxm, double dxp,
-                                                 double cs_edge, long long o0, long long o1, long long o2,
-                                                 long long o3)
+                                                 double cs_edge, int o0, int o1, int o2, int o3)
 {
     dvdots = pmin(0.0, dvdots);
     double rv1 = rho_v[o1], rv2 = rho_v[o2];

@@ -95,9 +95,9 @@ extern "C" int sams_lare_step_noalloc(const sams_lare_params *params, const sams
     g.ny = (int)p.ny;
     g.nz = (int)p.nz;
     g.zoff = 2;
-    g.sy = p.nz + 5;
-    g.sx = (p.ny + 5) * g.sy;
-    g.nelem = (p.nx + 5) * g.sx;
+    g.sy = (int)(p.nz + 5);
+    g.sx = (int)((p.ny + 5) * (p.nz + 5));
+    g.nelem = (p.nx + 5) * (p.ny + 5) * (p.nz + 5);
     const unsigned long long axis_len[3] = {(unsigned long long)p.nx + 6, (unsigned long long)p.ny + 6,
                                             (unsigned long long)p.nz + 6};
     const unsigned long long scratch_elems = (unsigned long long)sams::NSCRATCH * (unsigned long long)g.nelem;

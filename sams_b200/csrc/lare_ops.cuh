@@ -90,7 +90,7 @@ __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int
 // Sound speed on cells; with resistive MHD also keeps p_e, which the
 // predictor needs from before the Ohmic heating (lagran.cpp:121, 606).
 struct CellPrep {
-    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
@@ -98,7 +98,7 @@ struct CellPrep {
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long o = LOFF(i, j, k);
+        const int o = LOFF(i, j, k);
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         double bx1 = 0.5 * (bx[o] + bx[o - g.sx]);
         double by1 = 0.5 * (by[o] + by[o - g.sy]);
@@ -129,8 +129,8 @@ struct NodePrep {
         const int ip = i + 1, jp = j + 1, kp = k + 1;
         double cv0 = cv_at(c, i, j, k), cv1 = cv_at(c, ip, j, k), cv2 = cv_at(c, i, jp, k), cv3 = cv_at(c, ip, jp, k);
         double cv4 = cv_at(c, i, j, kp), cv5 = cv_at(c, ip, j, kp), cv6 = cv_at(c, i, jp, kp), cv7 = cv_at(c, ip, jp, kp);
-        long long o0 = LOFF(i, j, k), o1 = LOFF(ip, j, k), o2 = LOFF(i, jp, k), o3 = LOFF(ip, jp, k);
-        long long o4 = LOFF(i, j, kp), o5 = LOFF(ip, j, kp), o6 = LOFF(i, jp, kp), o7 = LOFF(ip, jp, kp);
+        int o0 = LOFF(i, j, k), o1 = LOFF(ip, j, k), o2 = LOFF(i, jp, k), o3 = LOFF(ip, jp, k);
+        int o4 = LOFF(i, j, kp), o5 = LOFF(ip, j, kp), o6 = LOFF(i, jp, kp), o7 = LOFF(ip, jp, kp);
         double sum_rho_cv = rho[o0] * cv0 + rho[o1] * cv1 + rho[o2] * cv2 + rho[o3] * cv3 +
                             rho[o4] * cv4 + rho[o5] * cv5 + rho[o6] * cv6 + rho[o7] * cv7;
         double sum_cv = cv0 + cv1 + cv2 + cv3 + cv4 + cv5 + cv6 + cv7;
@@ -145,7 +145,7 @@ struct NodePrep {
 // Edge viscosities.  dt is the previous step's (the CFL reduction of this
 // step runs later, lagran.cpp:155-156).
 struct Alpha {
-    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
@@ -156,26 +156,26 @@ struct Alpha {
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const RO rho_v{c.s[S_RHOV]}, cs_v{c.s[S_CSV]};
         const double dt = c.sc->dt, visc1 = c.p.visc1, v2n = c.p.visc2_norm;
-        const long long o = LOFF(i, j, k);
+        const int o = LOFF(i, j, k);
         if (i >= 0 && j >= 0) {  // alpha1: (0..nx+1, 0..ny+2, 0..nz+2)
-            long long o1 = LOFF(i - 1, j - 1, k - 1), o2 = LOFF(i, j - 1, k - 1);
-            long long o0 = o1 - g.sx, o3 = o2 + g.sx;
+            int o1 = LOFF(i - 1, j - 1, k - 1), o2 = LOFF(i, j - 1, k - 1);
+            int o0 = o1 - g.sx, o3 = o2 + g.sx;
             double dx = c.ax.dxb[i + 2], dxp = c.ax.dxb[i + 3], dxm = c.ax.dxb[i + 1];
             double dvdots = -(vx[o1] - vx[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A1][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
         }
         if (j >= 0 && j <= g.ny + 1) {  // alpha2: (-1..nx+1, 0..ny+1, 0..nz+2)
-            long long o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
-            long long o0 = o1 - g.sy, o3 = o2 + g.sy;
+            int o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
+            int o0 = o1 - g.sy, o3 = o2 + g.sy;
             double dx = c.ax.dyb[j + 2], dxp = c.ax.dyb[j + 3], dxm = c.ax.dyb[j + 1];
             double dvdots = -(vy[o1] - vy[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A2][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
         }
         if (j <= g.ny + 1 && k <= g.nz + 1) {  // alpha3: (-1..nx+1, -1..ny+1, 0..nz+1)
-            long long o1 = o - 1, o2 = o;
-            long long o0 = o1 - 1, o3 = o2 + 1;
+            int o1 = o - 1, o2 = o;
+            int o0 = o1 - 1, o3 = o2 + 1;
             double dx = c.ax.dzb[k + 2], dxp = c.ax.dzb[k + 3], dxm = c.ax.dzb[k + 1];
             double dvdots = -(vz[o1] - vz[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
@@ -188,7 +188,7 @@ struct Alpha {
 // cell's CFL candidate (p_visc is consumed here and never stored).
 // Returns the candidate (DBL_MAX outside the CFL range).
 struct Visc {
-    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
@@ -201,13 +201,13 @@ struct Visc {
         const Geom &g = c.g;
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
-        const long long SX = g.sx, SY = g.sy;
-        const long long o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy;
+        const int o = LOFF(i, j, k);
         const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
 #define DV2(a, b) ((vx[a] - vx[b]) * (vx[a] - vx[b]) + (vy[a] - vy[b]) * (vy[a] - vy[b]) + (vz[a] - vz[b]) * (vz[a] - vz[b]))
         // cell (ix, iy, iz) corners: m = minus one along that axis
-        const long long c_mmm = o - SX - SY - 1, c_0mm = o - SY - 1, c_00m = o - 1, c_m0m = o - SX - 1;
-        const long long c_mm0 = o - SX - SY, c_0m0 = o - SY, c_000 = o, c_m00 = o - SX;
+        const int c_mmm = o - SX - SY - 1, c_0mm = o - SY - 1, c_00m = o - 1, c_m0m = o - SX - 1;
+        const int c_mm0 = o - SX - SY, c_0m0 = o - SY, c_000 = o, c_m00 = o - SX;
         double a1 = DV2(c_mmm, c_0mm);
         double a2 = DV2(c_0mm, c_00m);
         double a3 = DV2(c_00m, c_m0m);
@@ -306,7 +306,7 @@ struct ResistRK {
     {
         const Geom &g = c.g;
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dxc = c.ax.dxc[i + 2], dyc = c.ax.dyc[j + 2], dzc = c.ax.dzc[k + 2];
         double jx1 = (bz[o + SY] - bz[o]) / dyc - (by[o + 1] - by[o]) / dzc;
         double jx2 = (bz[o + SX + SY] - bz[o + SX]) / dyc - (by[o + SX + 1] - by[o + SX]) / dzc;
@@ -336,7 +336,7 @@ struct ResistB {
     __device__ static void run(const Ctx &c, int last, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
         const RO fx{c.s[S_FLUXX]}, fy{c.s[S_FLUXY]}, fz{c.s[S_FLUXZ]};
         const double dt = c.sc->dt_sub;
@@ -381,7 +381,7 @@ struct Pred1 {
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const double dt = c.sc->dt;
         const double dxb0 = c.ax.dxb[i + 2], dxbm = c.ax.dxb[i + 1];
@@ -391,7 +391,7 @@ struct Pred1 {
         const double dyab0 = dxb0 * dzb0, dyabm = dxb0 * dzb0;          // dyab(j) and dyab(j-1)
         const double dzab0 = dxb0 * dyb0, dzabm = dxb0 * dyb0;          // dzab(k) and dzab(k-1)
         (void)dxbm; (void)dybm; (void)dzbm;
-        const long long a = o, am = o - SX, bm = o - SY, cm = o - 1;
+        const int a = o, am = o - SX, bm = o - SY, cm = o - 1;
         double vxb = 0.25 * (vx[a] + vx[bm] + vx[cm] + vx[bm - 1]);
         double vxbm = 0.25 * (vx[am] + vx[am - SY] + vx[am - 1] + vx[am - SY - 1]);
         double vyb = 0.25 * (vy[a] + vy[am] + vy[cm] + vy[am - 1]);
@@ -466,7 +466,7 @@ struct Pred1 {
 // Predictor, part 2: pressure and J x B forces on nodes and the half-step
 // velocity (lagran.cpp:619-733, Cartesian).
 struct Pred2 {
-    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
@@ -474,12 +474,12 @@ struct Pred2 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO pe{c.s[S_PE]}, pi{c.s[S_PI]}, cv1{c.s[S_CV1]};
         const RO bx1{c.s[S_B1X]}, by1{c.s[S_B1Y]}, bz1{c.s[S_B1Z]};
         const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
         const double dhy = dy, dhz = dz;
-        const long long q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
+        const int q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
                         qyz = o + SY + 1, qxyz = o + SX + SY + 1;
         double pp = pe[q0] + pi[q0], ppx = pe[qx] + pi[qx], ppy = pe[qy] + pi[qy], ppz = pe[qz] + pi[qz];
         double ppxy = pe[qxy] + pi[qxy], ppxz = pe[qxz] + pi[qxz], ppyz = pe[qyz] + pi[qyz], ppxyz = pe[qxyz] + pi[qxyz];
@@ -552,13 +552,13 @@ struct Corr1 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
         const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
 #define DD(a, b) (1 * ((vx[a] - vx[b]) * (vx1[a] - vx1[b]) + (vy[a] - vy[b]) * (vy1[a] - vy1[b]) + \
                        (vz[a] - vz[b]) * (vz1[a] - vz1[b])))
-        const long long mm0 = o - SX - SY, m00 = o - SX, om0 = o - SY;
+        const int mm0 = o - SX - SY, m00 = o - SX, om0 = o - SY;
         double a1 = DD(mm0, om0);
         double a2 = DD(om0, o);
         double a3 = DD(o, m00);
@@ -593,7 +593,7 @@ struct Corr2 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
         {
             const double rho_v = __ldg(c.s[S_RHOV] + o);
@@ -604,7 +604,7 @@ struct Corr2 {
         }
         if (i < 1 || j < 1 || k < 1) return;
         const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
-        const long long a = o, am = o - SX, bm = o - SY, cm = o - 1;
+        const int a = o, am = o - SX, bm = o - SY, cm = o - 1;
         double vxb = 0.25 * (vx1[a] + vx1[bm] + vx1[cm] + vx1[bm - 1]);
         double vxbm = 0.25 * (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]);
         double vyb = 0.25 * (vy1[a] + vy1[am] + vy1[cm] + vy1[am - 1]);
@@ -640,7 +640,7 @@ struct BScale {
     __device__ static void run(const Ctx &c, int back, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long o = LOFF(i, j, k);
+        const int o = LOFF(i, j, k);
         if (j >= -1 && k >= -1) {
             double a = dxab_at(c, i, j, k);
             double *b = c.f[SAMS_F_BX];
@@ -659,7 +659,7 @@ struct BScale {
     }
 };
 
-__device__ __forceinline__ long long dir_stride(const Geom &g, int dir)
+__device__ __forceinline__ int dir_stride(const Geom &g, int dir)
 {
     return dir == 0 ? g.sx : (dir == 1 ? g.sy : 1);
 }
@@ -679,11 +679,11 @@ struct SweepVol {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
         const double dxb0 = c.ax.dxb[i + 2], dyb0 = c.ax.dyb[j + 2], dzb0 = c.ax.dzb[k + 2];
         const double vol = dxb0 * (dyb0 * dzb0);
-        const long long am = o - SX, bm = o - SY, cm = o - 1;
+        const int am = o - SX, bm = o - SY, cm = o - 1;
         double tx = 0.0, ty = 0.0, tz = 0.0, vxb = 0.0, vxbm = 0.0, vyb = 0.0, vybm = 0.0, vzb = 0.0, vzbm = 0.0;
         if (DIR == 0) {
             const RO vx1{c.f[SAMS_F_VX1]};
@@ -740,7 +740,7 @@ struct SweepCvc {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO cv1{c.s[S_R_CV1]};
         c.s[S_R_CVC1][o] = 0.125 * (cv1[o] + cv1[o + SX] + cv1[o + SY] + cv1[o + SX + SY] +
                                     cv1[o + 1] + cv1[o + SX + 1] + cv1[o + SY + 1] + cv1[o + SX + SY + 1]);
@@ -758,13 +758,13 @@ struct SweepCT {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const long long d = dir_stride(g, DIR);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO db1{c.s[S_R_DB1]}, cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
         const RO v1{c.f[SAMS_F_VX1 + DIR]};
         // transverse offsets of the two db1 samples averaged for each flux
-        long long t1, t2, va1, va2;
+        int t1, t2, va1, va2;
         RO b1, b2;
         if (DIR == 0) {        // vx_by (avg +y, v avg -z), vx_bz (avg +z, v avg -y)
             t1 = SY; va1 = -1; b1.p = c.f[SAMS_F_BY];
@@ -807,7 +807,7 @@ struct SweepCTUpd {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO f1{c.s[S_R_CT1]}, f2{c.s[S_R_CT2]};
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
         const bool xb = i >= 0, xc = i >= 1, yb = j >= 0, yc = j >= 1, zb = k >= 0, zc = k >= 1;
@@ -839,10 +839,10 @@ struct SweepCTUpd {
 // Node-average advection velocity of a cell face along the sweep
 // (x/y/z_mass_flux and x/y/z_energy_flux use the same 4-point sums).
 template <int DIR>
-__device__ __forceinline__ double face_velocity(const Ctx &c, long long o)
+__device__ __forceinline__ double face_velocity(const Ctx &c, int o)
 {
     const Geom &g = c.g;
-    const long long SX = g.sx, SY = g.sy;
+    const int SX = g.sx, SY = g.sy;
     if (DIR == 0) {
         const RO v{c.f[SAMS_F_VX1]};
         return (v[o] + v[o - SY] + v[o - 1] + v[o - SY - 1]) * 0.25;
@@ -872,8 +872,8 @@ struct SweepMass {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long o = LOFF(i, j, k);
-        const long long d = dir_stride(g, DIR);
+        const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const RO rho{c.f[SAMS_F_RHO]}, cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
         double v = face_velocity<DIR>(c, o);
         c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
@@ -902,8 +902,8 @@ struct SweepS6 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const long long d = dir_stride(g, DIR);
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
         const RO dm{c.f[SAMS_F_DM]};
@@ -950,7 +950,7 @@ struct SweepS6 {
 // Energy updates (1..n)^3 and the three momentum fluxes (times dm).
 template <int DIR>
 struct SweepS7 {
-    static constexpr int kMinBlocks = 5;  // blocks of 256 per SM (register cap), tuned on B200
+    static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, DIR == 0 ? -1 : 0, g.nx, DIR == 1 ? -1 : 0, g.ny, DIR == 2 ? -1 : 0, g.nz);
@@ -958,8 +958,8 @@ struct SweepS7 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long o = LOFF(i, j, k);
-        const long long d = dir_stride(g, DIR);
+        const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
         if (i >= 1 && j >= 1 && k >= 1) {
@@ -997,8 +997,8 @@ struct SweepS8 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const long long o = LOFF(i, j, k);
-        const long long d = dir_stride(g, DIR);
+        const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const RO rv{c.s[S_R_RVN]}, cvc1{c.s[S_R_CVC1]}, cv2n{c.s[S_R_CV2N]}, dmn{c.s[S_R_DMN]};
         const double rvo = rv[o], cvco = cvc1[o], cv2o = cv2n[o];
         const double rho_v1 = (rvo * cvco + dmn[o - d] - dmn[o]) / cv2o;

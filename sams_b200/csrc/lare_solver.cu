@@ -304,9 +304,14 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     g.nz = (int)p.nz;
     g.zoff = 3;
     const long long zrow = ((p.nz + 6) + 7) / 8 * 8;
-    g.sy = zrow;
-    g.sx = (long long)(p.ny + 5) * zrow;
-    g.nelem = (long long)(p.nx + 5) * g.sx;
+    const long long sx = (long long)(p.ny + 5) * zrow;
+    if ((long long)(p.nx + 5) * sx > INT32_MAX) {
+        err = "one array of this grid exceeds 2^31 elements";
+        return SAMS_ERR_UNSUPPORTED;
+    }
+    g.sy = (int)zrow;
+    g.sx = (int)sx;
+    g.nelem = (long long)(p.nx + 5) * sx;
     const long long narr = SAMS_NFIELDS + NSCRATCH;
     const size_t abytes = (size_t)narr * (size_t)g.nelem * sizeof(double);
     if ((rc = check(cudaMalloc(&arena_, abytes), "cudaMalloc(state)"))) return rc;
