@@ -16,6 +16,7 @@
 #include "lare_solver.cuh"
 #include "lare_ops.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -69,6 +70,22 @@ __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
         double m = wmin[0];
         for (int w = 1; w < kThreads / 32; ++w) m = dev::pmin(m, wmin[w]);
         if (m < DBL_MAX) atomicMin(&c.sc->dtmin_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Dense box buffer <-> padded device rows (to_padded = 1: dense -> padded).
+__global__ void k_repack(const double *__restrict__ src, double *__restrict__ dst, Geom g, int to_padded)
+{
+    const long long n = (long long)(g.nx + 5) * (g.ny + 5) * (g.nz + 5);
+    const int ez = g.nz + 5;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t / ez;
+        const long long p = row * g.sy + (g.zoff - 2) + (t - row * ez);
+        if (to_padded)
+            dst[p] = src[t];
+        else
+            dst[t] = src[p];
     }
 }
 
@@ -243,10 +260,12 @@ void Solver::free_all()
     if (arena_) cudaFree(arena_);
     if (axes_) cudaFree(axes_);
     if (sc_) cudaFree(sc_);
+    if (staging_) cudaFree(staging_);
     if (own_stream_) cudaStreamDestroy(own_stream_);
     arena_ = nullptr;
     axes_ = nullptr;
     sc_ = nullptr;
+    staging_ = nullptr;
     own_stream_ = nullptr;
 }
 
@@ -295,6 +314,8 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
             }
     int rc;
     if ((rc = check(cudaSetDevice(device), "cudaSetDevice"))) return rc;
+    if ((rc = check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "sm count")))
+        return rc;
     if ((rc = check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
     stream_ = own_stream_;
 
@@ -406,16 +427,38 @@ int Solver::set_stream(cudaStream_t s)
     return SAMS_OK;
 }
 
+// Box rows are (nz+5) doubles; device rows are padded to g.sy with the row
+// starting at offset zoff-2.  Copies from or to host memory go through a
+// dense device staging buffer (one contiguous transfer at full link speed)
+// and a repacking kernel; device-to-device copies are strided copies.
+int Solver::staging(double **out)
+{
+    if (!staging_) {
+        const size_t bytes = (size_t)(ctx_.g.nx + 5) * (ctx_.g.ny + 5) * (ctx_.g.nz + 5) * sizeof(double);
+        int rc;
+        if ((rc = check(cudaMalloc(&staging_, bytes), "cudaMalloc(staging)"))) return rc;
+        bytes_ += (long long)bytes;
+    }
+    *out = staging_;
+    return SAMS_OK;
+}
+
 int Solver::upload(int field, const double *src, cudaMemcpyKind kind)
 {
     if (field < 0 || field >= SAMS_NFIELDS || !src) { err = "invalid field or buffer"; return SAMS_ERR_INVALID; }
     const Geom &g = ctx_.g;
-    // box rows are (nz+5) doubles; device rows are padded to g.sy with the
-    // row starting at offset zoff-2.
     const size_t w = (size_t)(g.nz + 5) * sizeof(double);
     const size_t rows = (size_t)(g.nx + 5) * (size_t)(g.ny + 5);
     double *dst = ctx_.f[field] + (g.zoff - 2);
-    return check(cudaMemcpy2DAsync(dst, (size_t)g.sy * sizeof(double), src, w, w, rows, kind, stream_), "upload");
+    if (kind == cudaMemcpyDeviceToDevice)
+        return check(cudaMemcpy2DAsync(dst, (size_t)g.sy * sizeof(double), src, w, w, rows, kind, stream_), "upload");
+    double *st;
+    int rc;
+    if ((rc = staging(&st))) return rc;
+    if ((rc = check(cudaMemcpyAsync(st, src, w * rows, kind, stream_), "upload"))) return rc;
+    k_repack<<<(unsigned)std::min<long long>(ceil_div((long long)(w / sizeof(double) * rows), kThreads), 8L * sm_count_),
+               kThreads, 0, stream_>>>(st, ctx_.f[field], g, 1);
+    return check(cudaGetLastError(), "repack");
 }
 
 int Solver::download(int field, double *dst, cudaMemcpyKind kind)
@@ -425,7 +468,18 @@ int Solver::download(int field, double *dst, cudaMemcpyKind kind)
     const size_t w = (size_t)(g.nz + 5) * sizeof(double);
     const size_t rows = (size_t)(g.nx + 5) * (size_t)(g.ny + 5);
     const double *src = ctx_.f[field] + (g.zoff - 2);
-    int rc = check(cudaMemcpy2DAsync(dst, w, src, (size_t)g.sy * sizeof(double), w, rows, kind, stream_), "download");
+    int rc;
+    if (kind == cudaMemcpyDeviceToDevice) {
+        rc = check(cudaMemcpy2DAsync(dst, w, src, (size_t)g.sy * sizeof(double), w, rows, kind, stream_), "download");
+    } else {
+        double *st;
+        if ((rc = staging(&st))) return rc;
+        k_repack<<<(unsigned)std::min<long long>(ceil_div((long long)(w / sizeof(double) * rows), kThreads),
+                                                 8L * sm_count_),
+                   kThreads, 0, stream_>>>(ctx_.f[field], st, g, 0);
+        if ((rc = check(cudaGetLastError(), "repack"))) return rc;
+        rc = check(cudaMemcpyAsync(dst, st, w * rows, kind, stream_), "download");
+    }
     if (rc) return rc;
     return check(cudaStreamSynchronize(stream_), "download sync");
 }

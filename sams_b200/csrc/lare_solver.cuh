@@ -73,17 +73,20 @@ private:
     void bc_fill_dim(unsigned mask, int dim);
     bool all_periodic(unsigned mask) const;
     template <class Op> void launch(int arg);
+    int staging(double **out);
     void free_all();
 
     sams_lare_params p_{};
     BcTable bc_{};
     int device_ = 0;
+    int sm_count_ = 148;  // multiprocessors of device_ (grid sizing)
     cudaStream_t own_stream_ = nullptr;
     cudaStream_t stream_ = nullptr;
     Ctx ctx_{};
     double *arena_ = nullptr;
     double *axes_ = nullptr;
     Scalars *sc_ = nullptr;
+    double *staging_ = nullptr;  // dense box buffer for host transfers (on first use)
     long long bytes_ = 0;
     long long launches_ = 0;
     long long launches_per_step_ = 0;
