@@ -9,6 +9,7 @@
 // whole batch.
 #include "lare_batch.cuh"
 #include "lare_ops.cuh"
+#include "lare_bc.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -124,7 +125,6 @@ __device__ __forceinline__ int locate(const long long *off, int n, long long g)
     return lo;
 }
 
-__device__ __forceinline__ int fld_lb(int f, int d) { return field_half(f, d) ? -2 : -1; }
 
 // Composite periodic fill (see k_bc_periodic in lare_solver.cu) for every
 // live solve whose fields in `mask` are all-periodic.  The flat index walks
@@ -184,7 +184,8 @@ __global__ void kb_bc_periodic(const Ctx *__restrict__ ctxs, const int *__restri
 }
 
 // One (dimension, edge) of the fields in `mask` for every live solve (those
-// handled by the composite fill are skipped when skip_periodic is set).
+// handled by the composite fill are skipped when skip_periodic is set); the
+// point formula and the ordering rule of small dimensions are lare_bc.cuh's.
 __global__ void kb_bc_edge(const Ctx *__restrict__ ctxs, const BcTable *__restrict__ bcs, const int *__restrict__ live,
                            const unsigned *__restrict__ pfields, const long long *__restrict__ off, int nlive,
                            long long total, unsigned mask, int d, int e, int skip_periodic, int resistive_only)
@@ -199,53 +200,18 @@ __global__ void kb_bc_edge(const Ctx *__restrict__ ctxs, const BcTable *__restri
         const BcTable &bt = bcs[inst];
         const long long t = gi - off[li];
         const Geom &g = c.g;
-        const int n[3] = {g.nx, g.ny, g.nz};
         for (int f = 0; f < SAMS_NFIELDS; ++f) {
             if (!(mask & (1u << f))) continue;
             const int kind = bt.kind[f][d][e];
             if (kind == SAMS_BC_NONE) continue;
-            int lo[3], hi[3];
-            for (int q = 0; q < 3; ++q) {
-                lo[q] = fld_lb(f, q);
-                hi[q] = n[q] + 2;
-            }
-            const bool half = field_half(f, d) != 0;
-            const int dlb = half ? 0 : 1, dub = n[d];
-            const int glo = e == 0 ? lo[d] : (half ? n[d] : n[d] + 1);
-            const int ghi = e == 0 ? 0 : n[d] + 2;
-            const int cnt = ghi - glo + 1;
-            lo[d] = glo;
-            hi[d] = ghi;
-            const int e1 = hi[1] - lo[1] + 1, e2 = hi[2] - lo[2] + 1;
-            if (t >= (long long)(hi[0] - lo[0] + 1) * e1 * e2) continue;
+            const BcEdge sl = bc_edge_slab(g, f, d, e);
+            const int e1 = sl.hi[1] - sl.lo[1] + 1, e2 = sl.hi[2] - sl.lo[2] + 1;
+            if (t >= (long long)(sl.hi[0] - sl.lo[0] + 1) * e1 * e2) continue;
             int q[3];
-            q[0] = lo[0] + (int)(t / ((long long)e1 * e2));
-            q[1] = lo[1] + (int)((t / e2) % e1);
-            q[2] = lo[2] + (int)(t % e2);
-            const int gq = q[d];
-            int s[3] = {q[0], q[1], q[2]};
-            double *a = c.f[f];
-            double v;
-            if (kind == SAMS_BC_PERIODIC) {
-                s[d] = e == 0 ? dub - cnt + 1 + (gq - glo) : dlb + (gq - glo);
-                v = a[box_off(g, s[0], s[1], s[2])];
-            } else if (kind == SAMS_BC_ZERO_GRADIENT) {
-                s[d] = e == 0 ? dlb : dub;
-                v = a[box_off(g, s[0], s[1], s[2])];
-            } else if (kind == SAMS_BC_MIRROR) {
-                const int last = e == 0 ? dlb : dub;
-                const int first = e == 0 ? ghi : glo;
-                int lt[3] = {q[0], q[1], q[2]};
-                lt[d] = last;
-                double av = a[box_off(g, lt[0], lt[1], lt[2])];
-                double bv = (av + av) / 2.0;
-                s[d] = last - (gq - first);
-                double delta = a[box_off(g, s[0], s[1], s[2])] - bv;
-                v = bv - delta;
-            } else {
-                v = bt.value[f][d][e];
-            }
-            a[box_off(g, q[0], q[1], q[2])] = v;
+            q[0] = sl.lo[0] + (int)(t / ((long long)e1 * e2));
+            q[1] = sl.lo[1] + (int)((t / e2) % e1);
+            q[2] = sl.lo[2] + (int)(t % e2);
+            bc_edge_apply(c.f[f], g, sl, kind, bt.value[f][d][e], d, e, q);
         }
     }
 }
@@ -375,7 +341,8 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
                 s.bc.value[f][d][e] = bcs.value[f][d][e];
                 per = per && k == SAMS_BC_PERIODIC;
             }
-        if (per) s.periodic_groups |= 1u << f;
+        // the one-pass periodic gather needs every source inside the domain
+        if (per && std::min(p.nx, std::min(p.ny, p.nz)) >= kBcSequentialBelow) s.periodic_groups |= 1u << f;
     }
     Geom g = batch_geom(p);
     const size_t abytes = (size_t)(SAMS_NFIELDS + NSCRATCH) * (size_t)g.nelem * sizeof(double);

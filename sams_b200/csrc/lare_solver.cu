@@ -15,6 +15,7 @@
 // Nothing is read back to the host inside a step.
 #include "lare_solver.cuh"
 #include "lare_ops.cuh"
+#include "lare_bc.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -174,66 +175,23 @@ __global__ void __launch_bounds__(kThreads) k_bc_periodic(Ctx c, FieldList fl)
 }
 
 // One (dimension, edge) of the given fields, exactly as the reference's
-// boundary-condition objects apply it.
+// boundary-condition objects apply it (lare_bc.cuh).
 __global__ void __launch_bounds__(kThreads) k_bc_edge(Ctx c, FieldList fl, BcTable bt, int d, int e)
 {
     const int f = fl.id[blockIdx.y];
     const int kind = bt.kind[f][d][e];
     if (kind == SAMS_BC_NONE) return;
     const Geom &g = c.g;
-    const int n[3] = {g.nx, g.ny, g.nz};
-    int lo[3], hi[3];
-    for (int q = 0; q < 3; ++q) {
-        lo[q] = field_lb(f, q);
-        hi[q] = n[q] + 2;
-    }
-    const bool half = field_half(f, d) != 0;
-    const int dlb = half ? 0 : 1, dub = n[d];
-    const int glo = e == 0 ? lo[d] : (half ? n[d] : n[d] + 1);
-    const int ghi = e == 0 ? 0 : n[d] + 2;
-    const int cnt = ghi - glo + 1;
-    lo[d] = glo;
-    hi[d] = ghi;
-    const int e1 = hi[1] - lo[1] + 1, e2 = hi[2] - lo[2] + 1;
-    const long long total = (long long)(hi[0] - lo[0] + 1) * e1 * e2;
+    const BcEdge sl = bc_edge_slab(g, f, d, e);
+    const int e1 = sl.hi[1] - sl.lo[1] + 1, e2 = sl.hi[2] - sl.lo[2] + 1;
+    const long long total = (long long)(sl.hi[0] - sl.lo[0] + 1) * e1 * e2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     int q[3];
-    q[0] = lo[0] + (int)(t / ((long long)e1 * e2));
-    q[1] = lo[1] + (int)((t / e2) % e1);
-    q[2] = lo[2] + (int)(t % e2);
-    const int gq = q[d];
-    int s[3] = {q[0], q[1], q[2]};
-    double *a = c.f[f];
-    double v;
-    switch (kind) {
-    case SAMS_BC_PERIODIC:
-        s[d] = e == 0 ? dub - cnt + 1 + (gq - glo) : dlb + (gq - glo);
-        v = a[box_off(g, s[0], s[1], s[2])];
-        break;
-    case SAMS_BC_ZERO_GRADIENT:
-        s[d] = e == 0 ? dlb : dub;
-        v = a[box_off(g, s[0], s[1], s[2])];
-        break;
-    case SAMS_BC_MIRROR: {
-        const int last = e == 0 ? dlb : dub;
-        const int first = e == 0 ? ghi : glo;
-        int lt[3] = {q[0], q[1], q[2]};
-        lt[d] = last;
-        double av = a[box_off(g, lt[0], lt[1], lt[2])];
-        double bv = (av + av) / 2.0;
-        s[d] = last - (gq - first);
-        double delta = a[box_off(g, s[0], s[1], s[2])] - bv;
-        v = bv - delta;
-        break;
-    }
-    case SAMS_BC_CLAMP:
-        v = bt.value[f][d][e];
-        break;
-    default:
-        return;
-    }
-    a[box_off(g, q[0], q[1], q[2])] = v;
+    q[0] = sl.lo[0] + (int)(t / ((long long)e1 * e2));
+    q[1] = sl.lo[1] + (int)((t / e2) % e1);
+    q[2] = sl.lo[2] + (int)(t % e2);
+    bc_edge_apply(c.f[f], g, sl, kind, bt.value[f][d][e], d, e, q);
 }
 
 FieldList make_list(unsigned mask)
@@ -510,7 +468,8 @@ void Solver::bc_fill(unsigned mask)
     FieldList fl = make_list(mask);
     if (fl.n == 0) return;
     const Geom &g = ctx_.g;
-    if (all_periodic(mask)) {
+    // the one-pass gather needs every source inside the domain (n >= 3)
+    if (all_periodic(mask) && std::min(g.nx, std::min(g.ny, g.nz)) >= kBcSequentialBelow) {
         // the largest ghost shell is the all-half-cell one
         const long long e0 = g.nx + 5, e1 = g.ny + 5, e2 = g.nz + 5;
         const long long cnt = 5 * e1 * e2 + (long long)g.nx * 5 * e2 + (long long)g.nx * g.ny * 5;

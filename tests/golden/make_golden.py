@@ -29,6 +29,11 @@ CASES = [
     ("ot_b0_10x10x4_s4", "ot", 10, 10, 4, 4, 1, 0.9 / (4 * np.pi) ** 0.5),
     ("rf_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0),
     ("harris_12x10x6_s4", "harris", 12, 10, 6, 4, 3, 0.0),
+    # dimensions with fewer than three cells: 2.5-D (the reference's own
+    # Orszag-Tang runs nz = 2) and 2-D; edge copies read their own output here
+    ("ot_12x10x2_s4", "ot", 12, 10, 2, 4, 1, 0.0),
+    ("ot_8x6x1_s3", "ot", 8, 6, 1, 3, 1, 0.0),
+    ("harris_10x2x4_s3", "harris", 10, 2, 4, 3, 3, 0.0),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 

@@ -48,3 +48,31 @@ def test_runner_gpu_matches_oracle(runner_bin, nsteps, shape):
     rc, out = _run(runner_bin, "--run", nsteps, *shape)
     assert rc == 0, out
     assert '"mismatches": 0' in out and '"time_ok": true' in out, out
+
+
+# the reference tree, read in place (the same default as oracle/Makefile's REF)
+REF_OT = os.path.join(os.environ.get("SAMS_REFERENCE_TREE", "/root/reference"), "src", "InitialConditions", "OrszagTang")
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_OT), reason="reference tree not present on this machine")
+def test_reference_ic_package_compiles_and_sets_up(tmp_path):
+    """The reference's own Orszag-Tang IC package, compiled unchanged from its
+    tree against include/sams/ (its includes of harness.h, runner.h,
+    shared_data.h and builtInBoundaryConditions.h resolve to one-line shims),
+    sets up a runner on the host: 128 x 128 x 2, gamma = 5/3, every variable
+    periodic on every edge, fields as the package writes them."""
+    from sams_b200 import build as sb
+    lib = sb.build()
+    shim = tmp_path / "shim"
+    shim.mkdir()
+    for h in ("harness.h", "runner.h", "shared_data.h", "builtInBoundaryConditions.h"):
+        (shim / h).write_text('#include "sams/lare3d.hpp"\n')
+    exe = str(tmp_path / "ref_ic")
+    cmd = ["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"), "-I", str(shim), "-I", REF_OT,
+           os.path.join(ROOT, "tests", "cpp", "reference_ic_setup.cpp"), os.path.join(REF_OT, "OrszagTang.cpp"),
+           "-o", exe, "-L", os.path.dirname(lib), "-lsams_lare", "-Wl,-rpath," + os.path.dirname(lib)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    rc, out = _run(exe)
+    assert rc == 0, out
+    assert '"nx": 128, "ny": 128, "nz": 2' in out and '"periodic_slots": 78' in out, out

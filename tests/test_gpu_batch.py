@@ -10,7 +10,8 @@ pytestmark = pytest.mark.gpu
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 
 MIX = [("ot", (16, 12, 4), 1, 0.0), ("ot", (24, 24, 4), 2, 0.9 / (4 * np.pi) ** 0.5),
-       ("rf", (12, 12, 12), 3, 0.0), ("harris", (16, 12, 6), 4, 0.0), ("ot", (40, 8, 5), 5, 0.0)]
+       ("rf", (12, 12, 12), 3, 0.0), ("harris", (16, 12, 6), 4, 0.0), ("ot", (40, 8, 5), 5, 0.0),
+       ("ot", (20, 16, 2), 6, 0.0), ("rf", (10, 2, 8), 7, 0.0)]
 
 
 def _solo(case, n, seed, b0, steps):

@@ -52,6 +52,9 @@ def test_gpu_matches_reference_golden(name):
     ("rf", (16, 16, 16), 10),
     ("rf", (20, 12, 9), 6),
     ("harris", (24, 16, 8), 10),
+    ("rf", (8, 8, 2), 5),          # fewer than three cells in z: ordered edge copies
+    ("ot", (2, 9, 5), 5),          # ... in x
+    ("harris", (12, 1, 6), 4),     # ... one cell in y, walls
 ])
 def test_gpu_matches_checker(case, n, steps, oracle_lib):
     lo = oracle_lib

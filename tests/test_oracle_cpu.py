@@ -37,7 +37,8 @@ def test_checker_matches_reference_golden(name, oracle_lib):
 
 
 @pytest.mark.skipif(not os.path.exists(lo.REF_BIN), reason="reference harness binary not built here")
-@pytest.mark.parametrize("case,n,steps", [("ot", (9, 11, 5), 12), ("rf", (8, 8, 8), 6), ("harris", (10, 8, 4), 6)])
+@pytest.mark.parametrize("case,n,steps", [("ot", (9, 11, 5), 12), ("rf", (8, 8, 8), 6), ("harris", (10, 8, 4), 6),
+                                          ("rf", (8, 8, 2), 3), ("ot", (2, 9, 5), 3)])
 def test_checker_matches_reference_binary(case, n, steps, tmp_path, oracle_lib):
     from oracle.dumpio import Dump
     nx, ny, nz = n

@@ -34,7 +34,7 @@ def _noalloc_fn():
 
 
 @pytest.mark.parametrize("case,n,calls", [("ot", (24, 20, 8), (3, 2)), ("rf", (16, 14, 12), (2, 2)),
-                                          ("harris", (20, 12, 6), (2, 3))])
+                                          ("harris", (20, 12, 6), (2, 3)), ("ot", (16, 12, 2), (2, 2))])
 def test_noalloc_matches_regular_entry_point(case, n, calls):
     import torch
 
