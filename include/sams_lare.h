@@ -74,6 +74,20 @@ int sams_lare_set_bc(sams_lare_solver *h, int field, int dim, int edge,
 int sams_lare_upload_field(sams_lare_solver *h, int field, const double *host_box);
 int sams_lare_download_field(sams_lare_solver *h, int field, double *host_box);
 
+/* Checkpoint / restart.  save writes the 13 harness variables over their
+ * local ranges, the step count, the time and the last step's dt (which the
+ * next step's edge viscosity reads) as a SAMSDUMP1 file: a text magic line,
+ * a one-line JSON header with an array directory, then little-endian float64
+ * arrays -- the dump format the oracle's reference harness writes for the
+ * reference's own state (the reference itself writes no field data,
+ * src/PhysicsPackages/LARE/io/writerSimple.h:151).  load reads such a file of the same grid
+ * (the nine state fields must be present; extra arrays are skipped), so a
+ * run resumes bit for bit, also from a state the reference produced.
+ * Replaces the runner's output/restart hooks (include/runner/runner.h:505-525)
+ * for this path.  Both synchronise the solver's stream. */
+int sams_lare_save(sams_lare_solver *h, const char *path);
+int sams_lare_load(sams_lare_solver *h, const char *path);
+
 /* Same, from / to a device box buffer (e.g. a CUDA tensor's storage). */
 int sams_lare_upload_field_device(sams_lare_solver *h, int field, const double *dev_box);
 int sams_lare_download_field_device(sams_lare_solver *h, int field, double *dev_box);
@@ -163,7 +177,8 @@ enum sams_serve_status {
     SAMS_SERVE_QUEUED = 0,
     SAMS_SERVE_RUNNING = 1,
     SAMS_SERVE_DONE = 2,
-    SAMS_SERVE_FAILED = 3
+    SAMS_SERVE_FAILED = 3,
+    SAMS_SERVE_CANCELLED = 4
 };
 
 typedef struct sams_lare_serve_stats {
@@ -194,7 +209,12 @@ int sams_lare_serve_set_max_cells(sams_lare_server *s, int64_t max_cells);
 int sams_lare_serve_poll(sams_lare_server *s, int64_t ticket, int *status, double *latency_s);
 /* Copy one of the nine kept result fields (index as for out[]). */
 int sams_lare_serve_fetch(sams_lare_server *s, int64_t ticket, int state_index, double *host_box);
-/* Forget a finished request (frees a kept result). */
+/* Withdraw a request: a queued one leaves the queue at once; a running one
+ * is retired (its device memory freed, no result) before the scheduler's
+ * next step, after which its status is SAMS_SERVE_CANCELLED.  A request that
+ * already finished is refused with SAMS_ERR_INVALID. */
+int sams_lare_serve_cancel(sams_lare_server *s, int64_t ticket);
+/* Forget a finished or cancelled request (frees a kept result). */
 int sams_lare_serve_release(sams_lare_server *s, int64_t ticket);
 /* Wait until nothing is queued or running (SAMS_ERR_TIMEOUT otherwise). */
 int sams_lare_serve_drain(sams_lare_server *s, double timeout_s);

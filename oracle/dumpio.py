@@ -11,6 +11,26 @@ import json
 import numpy as np
 
 
+def write(path, header, arrays):
+    """Write a SAMSDUMP1 file: `header` (dict without "arrays") plus the
+    named arrays as (array, lower_bounds) pairs, each over its own bounds."""
+    entries, blobs, off = [], [], 0
+    for name, (arr, lb) in arrays.items():
+        arr = np.ascontiguousarray(arr, dtype="<f8")
+        ub = [l + s - 1 for l, s in zip(lb, arr.shape)]
+        entries.append({"name": name, "rank": arr.ndim, "lb": list(lb) + [0] * (3 - arr.ndim),
+                        "ub": ub + [0] * (3 - arr.ndim), "offset": off})
+        blobs.append(arr.tobytes())
+        off += arr.nbytes
+    h = dict(header)
+    h["arrays"] = entries
+    with open(path, "wb") as f:
+        f.write(b"SAMSDUMP1\n")
+        f.write(json.dumps(h, separators=(",", ":")).encode() + b"\n")
+        for b in blobs:
+            f.write(b)
+
+
 class Dump:
     def __init__(self, path):
         with open(path, "rb") as f:

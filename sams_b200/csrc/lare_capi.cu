@@ -2,10 +2,12 @@
 // sams::Solver.
 #include "sams_lare.h"
 #include "lare_solver.cuh"
+#include "lare_dump.cuh"
 
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 struct sams_lare_solver {
     sams::Solver s;
@@ -172,6 +174,50 @@ int sams_lare_device_bytes(sams_lare_solver *h, int64_t *bytes)
     if (!h || !bytes) return fail(SAMS_ERR_INVALID, "invalid argument");
     *bytes = h->s.device_bytes();
     return SAMS_OK;
+}
+
+int sams_lare_save(sams_lare_solver *h, const char *path)
+{
+    if (!h || !path) return fail(SAMS_ERR_INVALID, "sams_lare_save: null argument");
+    const sams::Geom &g = h->s.geom();
+    const size_t n = (size_t)(g.nx + 5) * (g.ny + 5) * (g.nz + 5);
+    std::vector<std::vector<double>> bufs(SAMS_NFIELDS, std::vector<double>(n));
+    const double *box[SAMS_NFIELDS];
+    int rc;
+    for (int f = 0; f < SAMS_NFIELDS; ++f) {
+        if ((rc = h->s.download(f, bufs[f].data(), cudaMemcpyDefault))) return pass(h, rc);
+        box[f] = bufs[f].data();
+    }
+    sams::Scalars sc;
+    if ((rc = h->s.scalars(sc))) return pass(h, rc);
+    sams::DumpState st{g.nx, g.ny, g.nz, sc.step, sc.time, sc.dt};
+    std::string err;
+    if ((rc = sams::dump_write(path, st, box, err))) return fail(rc, "sams_lare_save: " + err);
+    return SAMS_OK;
+}
+
+int sams_lare_load(sams_lare_solver *h, const char *path)
+{
+    if (!h || !path) return fail(SAMS_ERR_INVALID, "sams_lare_load: null argument");
+    const sams::Geom &g = h->s.geom();
+    const size_t n = (size_t)(g.nx + 5) * (g.ny + 5) * (g.nz + 5);
+    std::vector<std::vector<double>> bufs(SAMS_NFIELDS, std::vector<double>(n, 0.0));
+    double *box[SAMS_NFIELDS];
+    for (int f = 0; f < SAMS_NFIELDS; ++f) box[f] = bufs[f].data();
+    bool present[SAMS_NFIELDS];
+    sams::DumpState st{g.nx, g.ny, g.nz, 0, 0.0, 0.0};
+    std::string err;
+    int rc = sams::dump_read(path, st, box, present, err);
+    if (rc) return fail(rc, "sams_lare_load: " + err);
+    const int state[9] = {SAMS_F_RHO, SAMS_F_ENERGY_ELECTRON, SAMS_F_ENERGY_ION, SAMS_F_VX, SAMS_F_VY,
+                          SAMS_F_VZ, SAMS_F_BX, SAMS_F_BY, SAMS_F_BZ};
+    for (int f : state)
+        if (!present[f])
+            return fail(SAMS_ERR_INVALID, std::string("sams_lare_load: ") + path + " lacks state field " +
+                                              sams_lare_field_names[f]);
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        if (present[f] && (rc = h->s.upload(f, box[f], cudaMemcpyDefault))) return pass(h, rc);
+    return pass(h, h->s.set_scalars(st.dt, st.time, st.step));
 }
 
 int sams_lare_phase_times(sams_lare_solver *h, double ms[5])

@@ -46,6 +46,7 @@ struct Request {
     long long cells = 0;
     int slot = -1;
     int status = SAMS_SERVE_QUEUED;
+    bool cancel = false;  // set by sams_lare_serve_cancel while running
     long long bytes = 0;
     Clock::time_point t_submit, t_admit, t_done;
 };
@@ -157,6 +158,23 @@ void sams_lare_server::loop()
             std::unique_lock<std::mutex> lk(mu);
             cv.wait(lk, [&] { return stop || !queue.empty() || !running.empty(); });
             if (stop) return;
+            // running solves cancelled since the last step leave before it
+            std::vector<Request *> keep;
+            for (Request *r : running) {
+                if (!r->cancel) {
+                    keep.push_back(r);
+                    continue;
+                }
+                batch.remove(r->slot);
+                in_use -= r->bytes;
+                cells_in_use -= r->cells;
+                r->status = SAMS_SERVE_CANCELLED;
+                r->t_done = Clock::now();
+            }
+            if (keep.size() != running.size()) {
+                running.swap(keep);
+                cv.notify_all();
+            }
             admit_locked();
         }
         if (running.empty()) continue;
@@ -293,7 +311,8 @@ int sams_lare_serve_poll(sams_lare_server *s, int64_t ticket, int *status, doubl
     Request *r = it->second.get();
     *status = r->status;
     if (latency_s)
-        *latency_s = (r->status == SAMS_SERVE_DONE || r->status == SAMS_SERVE_FAILED)
+        *latency_s = (r->status == SAMS_SERVE_DONE || r->status == SAMS_SERVE_FAILED ||
+                      r->status == SAMS_SERVE_CANCELLED)
                          ? std::chrono::duration<double>(r->t_done - r->t_submit).count()
                          : std::chrono::duration<double>(Clock::now() - r->t_submit).count();
     return SAMS_OK;
@@ -313,13 +332,40 @@ int sams_lare_serve_fetch(sams_lare_server *s, int64_t ticket, int state_index, 
     return SAMS_OK;
 }
 
+int sams_lare_serve_cancel(sams_lare_server *s, int64_t ticket)
+{
+    if (!s) return SAMS_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) {
+        sams_capi_set_last_error("sams_lare_serve_cancel: unknown ticket");
+        return SAMS_ERR_INVALID;
+    }
+    Request *r = it->second.get();
+    if (r->status == SAMS_SERVE_QUEUED) {
+        s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
+        r->status = SAMS_SERVE_CANCELLED;
+        r->t_done = Clock::now();
+        s->cv.notify_all();
+        return SAMS_OK;
+    }
+    if (r->status == SAMS_SERVE_RUNNING) {
+        r->cancel = true;  // the scheduler retires it before its next step
+        s->cv.notify_all();
+        return SAMS_OK;
+    }
+    sams_capi_set_last_error("sams_lare_serve_cancel: request already finished");
+    return SAMS_ERR_INVALID;
+}
+
 int sams_lare_serve_release(sams_lare_server *s, int64_t ticket)
 {
     if (!s) return SAMS_ERR_INVALID;
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->all.find(ticket);
     if (it == s->all.end()) return SAMS_ERR_INVALID;
-    if (it->second->status != SAMS_SERVE_DONE && it->second->status != SAMS_SERVE_FAILED) {
+    if (it->second->status != SAMS_SERVE_DONE && it->second->status != SAMS_SERVE_FAILED &&
+        it->second->status != SAMS_SERVE_CANCELLED) {
         sams_capi_set_last_error("sams_lare_serve_release: request still queued or running");
         return SAMS_ERR_INVALID;
     }

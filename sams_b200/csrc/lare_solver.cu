@@ -645,6 +645,20 @@ int Solver::sync()
     return SAMS_OK;
 }
 
+int Solver::set_scalars(double dt, double time, long long step)
+{
+    Scalars h{};
+    h.dt = dt;
+    h.dtr = dt;
+    h.time = time;
+    h.step = step;
+    const double big = DBL_MAX;
+    std::memcpy(&h.dtmin_bits, &big, sizeof big);
+    int rc = check(cudaMemcpyAsync(sc_, &h, sizeof(Scalars), cudaMemcpyHostToDevice, stream_), "scalars write");
+    if (rc) return rc;
+    return check(cudaStreamSynchronize(stream_), "scalars sync");
+}
+
 int Solver::scalars(Scalars &out)
 {
     int rc = check(cudaMemcpyAsync(&out, sc_, sizeof(Scalars), cudaMemcpyDeviceToHost, stream_), "scalars read");

@@ -53,6 +53,8 @@ public:
     int step_graph(long long nsteps);
     int sync();
     int scalars(Scalars &out);
+    // Restart: the dt of the last step taken, the time and the step count.
+    int set_scalars(double dt, double time, long long step);
     long long device_bytes() const { return bytes_; }
     long long launches_per_step() const { return launches_per_step_; }
     const Geom &geom() const { return ctx_.g; }

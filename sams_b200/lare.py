@@ -92,6 +92,8 @@ def lib():
     L.sams_lare_device_bytes.argtypes = [vp, ctypes.POINTER(i64)]
     L.sams_lare_launches_per_step.argtypes = [vp, ctypes.POINTER(i64)]
     L.sams_lare_phase_times.argtypes = [vp, _P]
+    L.sams_lare_save.argtypes = [vp, ctypes.c_char_p]
+    L.sams_lare_load.argtypes = [vp, ctypes.c_char_p]
     L.sams_lare_case_setup.argtypes = [ctypes.c_int, i64, i64, i64, ctypes.c_double,
                                        ctypes.POINTER(Params), ctypes.POINTER(Bcs)]
     L.sams_lare_case_fields.argtypes = [ctypes.c_int, ctypes.POINTER(Params), ctypes.c_uint64, ctypes.c_double,
@@ -190,6 +192,16 @@ class LARE3D:
             out = np.empty(self.shape)
         _check(lib().sams_lare_download_field(self._h, f, out.ctypes.data_as(_P)))
         return out
+
+    def save(self, path):
+        """Checkpoint: the 13 fields, step count, time and last dt as a
+        SAMSDUMP1 file (readable by oracle.dumpio.Dump)."""
+        _check(lib().sams_lare_save(self.handle, str(path).encode()))
+
+    def load(self, path):
+        """Restart from a SAMSDUMP1 file of the same grid (a checkpoint, or a
+        dump of the reference's own state)."""
+        _check(lib().sams_lare_load(self.handle, str(path).encode()))
 
     def step(self, n=1, graph=False):
         if graph:
@@ -359,7 +371,7 @@ class ServeStats(ctypes.Structure):
                 ("device_bytes_in_use", ctypes.c_int64)]
 
 
-SERVE_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+SERVE_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
 
 def _bind_serve(L):
@@ -373,6 +385,7 @@ def _bind_serve(L):
     L.sams_lare_serve_poll.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_int), _P]
     L.sams_lare_serve_fetch.argtypes = [vp, i64, ctypes.c_int, _P]
     L.sams_lare_serve_release.argtypes = [vp, i64]
+    L.sams_lare_serve_cancel.argtypes = [vp, i64]
     L.sams_lare_serve_drain.argtypes = [vp, ctypes.c_double]
     L.sams_lare_serve_get_stats.argtypes = [vp, ctypes.POINTER(ServeStats)]
     L.sams_lare_serve_destroy.argtypes = [vp]
@@ -431,6 +444,11 @@ class Server:
         out = np.empty(self._keep[ticket][2])
         _check(lib().sams_lare_serve_fetch(self._h, ticket, index, out.ctypes.data_as(_P)))
         return out
+
+    def cancel(self, ticket):
+        """Withdraw a queued or running request (its status becomes
+        "cancelled"; a running one leaves before the next batched step)."""
+        _check(lib().sams_lare_serve_cancel(self._h, ticket))
 
     def release(self, ticket):
         _check(lib().sams_lare_serve_release(self._h, ticket))

@@ -20,6 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import lare_oracle as lo  # noqa: E402
+from oracle import dumpio  # noqa: E402
 from oracle.dumpio import Dump  # noqa: E402
 
 # (name, case, nx, ny, nz, steps, seed, b0)
@@ -36,6 +37,11 @@ CASES = [
     ("harris_10x2x4_s3", "harris", 10, 2, 4, 3, 3, 0.0),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
+# (file, case, nx, ny, nz, steps, seed): the reference's full harness state
+# (13 variables, step, time, last dt) after `steps` steps as a SAMSDUMP1
+# restart file; ot_12x10x6_at3 continues to ot_12x10x6_s5 above.
+RESTARTS = [("ot_12x10x6_at3.dump", "ot", 12, 10, 6, 3, 1)]
+HARNESS = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "vx1", "vy1", "vz1", "bx", "by", "bz", "dm"]
 
 
 def main():
@@ -56,6 +62,15 @@ def main():
             out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
             print(name, "dt", d.header["dt"])
+    for fname, case, nx, ny, nz, steps, seed in RESTARTS:
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "d.dump")
+            lo.run_reference(case, nx, ny, nz, steps, path, seed=seed)
+            d = Dump(path)
+            header = {k: d.header[k] for k in ("nx", "ny", "nz", "step", "phase", "time", "dt", "dts")}
+            header["generator"] = "oracle/_ref/lare_ref (reference LARE3D), harness variables only"
+            dumpio.write(os.path.join(HERE, fname), header, {n: d.get(n) for n in HARNESS})
+            print(fname, "step", d.header["step"], "dt", d.header["dt"])
 
 
 def load(name):

@@ -76,3 +76,35 @@ def test_failed_solve_is_isolated_and_kept_results_fetchable():
         tiny.submit(p16, b16, lare.case_fields("rf", p16), 1)
     assert e.value.status == -7
     tiny.close()
+
+
+def test_cancel_queued_and_running_requests():
+    """A cap of one running 16^3 solve: the first request runs long, the
+    next two wait.  Cancelling the running one and one queued one leaves the
+    last to run alone, and its result still equals its solo run."""
+    srv = lare.Server(1 << 30, max_cells=16 * 16 * 16)
+    p, b = lare.case_setup("rf", 16, 16, 16)
+    long_run = srv.submit(p, b, lare.case_fields("rf", p, seed=1), 100000)
+    queued = srv.submit(p, b, lare.case_fields("rf", p, seed=2), 5)
+    out = [np.zeros(lare.box_shape(16, 16, 16)) for _ in range(9)]
+    last = srv.submit(p, b, lare.case_fields("rf", p, seed=3), 6, out)
+    for _ in range(2000):
+        if srv.poll(long_run)[0] == "running":
+            break
+        time.sleep(0.005)
+    assert srv.poll(queued)[0] == "queued"
+    srv.cancel(queued)
+    assert srv.poll(queued)[0] == "cancelled"
+    srv.cancel(long_run)
+    srv.drain(300)
+    assert srv.poll(long_run)[0] == "cancelled"
+    assert srv.poll(last)[0] == "done"
+    ref = _solo("rf", (16, 16, 16), 6, 3)
+    for q, f in enumerate(STATE):
+        sl = lare.field_slices(f, 16, 16, 16)
+        assert np.array_equal(out[q][sl], ref[f][sl]), f
+    with pytest.raises(lare.LareError):
+        srv.cancel(last)              # already finished
+    for t in (long_run, queued, last):
+        srv.release(t)
+    srv.close()
