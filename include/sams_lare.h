@@ -30,7 +30,7 @@ enum sams_status {
     SAMS_ERR_INVALID = -1,      /* bad argument or unsupported option      */
     SAMS_ERR_NOMEM = -2,        /* device or host allocation failed         */
     SAMS_ERR_CUDA = -3,         /* a CUDA runtime call failed               */
-    SAMS_ERR_UNSUPPORTED = -4,  /* geometry / rke / custom BC not built     */
+    SAMS_ERR_UNSUPPORTED = -4,  /* geometry or option not built            */
     SAMS_ERR_NONFINITE = -5,    /* the timestep became NaN or infinite      */
     SAMS_ERR_TIMEOUT = -6,      /* a bounded wait ran out                   */
     SAMS_ERR_BUDGET = -7        /* request exceeds the memory budget        */
@@ -51,7 +51,7 @@ const char *sams_lare_last_error(void);
  * (include/runner/runner.h:456-464).  Boundary conditions are copied; they
  * replace the IC package's setBoundaryConditions
  * (variableDef::addBoundaryCondition, include/harness/variableDef.h:402-481).
- * Supported: Cartesian geometry, rke = 0. */
+ * Supported: Cartesian geometry (rke on or off). */
 int sams_lare_create(const sams_lare_params *params, const sams_lare_bcs *bcs,
                      int device, sams_lare_solver **out);
 

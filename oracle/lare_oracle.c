@@ -39,6 +39,7 @@ struct lo_state {
     double *cs, *cs_v;
     /* remap temporaries (remapData.h:23-32) */
     double *rho1, *cv2, *cvc1, *db1, *r_rho_v, *rho_v1, *flux;
+    double *delta_ke; /* remap kinetic-energy correction (rke only, setup.cpp:251) */
     double dt, dtr, time, visc2_norm;
     int64_t step;
     double xpass, ypass, zpass;
@@ -996,6 +997,65 @@ static void sweep_volumes(lo_state *s, int dir)
     }
 }
 
+/* Kinetic-energy error of one momentum flux, added to delta_ke at the four
+ * nodes across the face (x_mom_flux xremap.cpp:534-558, y_mom_flux
+ * yremap.cpp:557-583, z_mom_flux zremap.cpp:513-536).  The reference adds
+ * with atomics inside its parallel loop; this is its serial order (source
+ * points in index order, the four adds in statement order), which is the
+ * reference's result with one thread.  flux holds the momentum flux before
+ * it is multiplied by dm; u the velocity component before its update. */
+static void rke_scatter(lo_state *s, int dir, const double *u)
+{
+    DIMS(s);
+    const int64_t d1 = dir == 0 ? (int64_t)sy * sz : (dir == 1 ? sz : 1);
+    const double *rv1 = s->rho_v1, *cv2 = s->cv2, *flux = s->flux, *dm = s->f[SAMS_F_DM];
+    double *dke = s->delta_ke;
+    const int64_t ihi = dir == 0 ? nx - 1 : nx, jhi = dir == 1 ? ny - 1 : ny, khi = dir == 2 ? nz - 1 : nz;
+    for (int64_t ix = 0; ix <= ihi; ++ix)
+        for (int64_t iy = 0; iy <= jhi; ++iy)
+            for (int64_t iz = 0; iz <= khi; ++iz) {
+                const int64_t o = I3(ix, iy, iz), op = o + d1, om = o - d1;
+                const double m = rv1[o] * cv2[o];
+                const double mp = rv1[op] * cv2[op];
+                const double ai = (u[o] - flux[om]) * dm[om] / m - (u[o] - flux[o]) * dm[o] / m;
+                const double aip = (u[op] - flux[o]) * dm[o] / mp - (u[op] - flux[op]) * dm[op] / mp;
+                double dk = (u[op] - u[o]) * (flux[o] - 0.5 * (u[op] + u[o])) - 0.5 * ai * (u[o] - flux[o]) +
+                            0.5 * aip * (u[op] - flux[o]);
+                dk = dk * dm[o] * 0.5;
+                if (dir == 0) {
+                    dke[I3(ix + 1, iy, iz)] += dk;
+                    dke[I3(ix + 1, iy + 1, iz)] += dk;
+                    dke[I3(ix + 1, iy + 1, iz + 1)] += dk;
+                    dke[I3(ix + 1, iy, iz + 1)] += dk;
+                } else if (dir == 1) {
+                    dke[I3(ix + 1, iy + 1, iz)] += dk;
+                    dke[I3(ix, iy + 1, iz)] += dk;
+                    dke[I3(ix + 1, iy + 1, iz + 1)] += dk;
+                    dke[I3(ix, iy + 1, iz + 1)] += dk;
+                } else {
+                    dke[I3(ix, iy, iz + 1)] += dk;
+                    dke[I3(ix + 1, iy, iz + 1)] += dk;
+                    dke[I3(ix, iy + 1, iz + 1)] += dk;
+                    dke[I3(ix + 1, iy + 1, iz + 1)] += dk;
+                }
+            }
+}
+
+/* energy_correction (diagnostics.cpp:125-135), after the remap (shared_data.h:414-417) */
+static void energy_correction(lo_state *s)
+{
+    DIMS(s);
+    double *ee = s->f[SAMS_F_ENERGY_ELECTRON], *ei = s->f[SAMS_F_ENERGY_ION];
+    const double *rho = s->f[SAMS_F_RHO], *cv = s->cv, *dke = s->delta_ke;
+    LOOP3(1, nx, 1, ny, 1, nz)
+    {
+        const int64_t o = I3(ix, iy, iz);
+        const double d = pmax(-dke[o], 0.0) / (rho[o] * cv[o]);
+        ee[o] += 0.5 * d;
+        ei[o] += 0.5 * d;
+    }
+}
+
 /* Offsets of +-1, +2 along a direction. */
 #define STEP_OF(dir) ((dir) == 0 ? sy * sz : ((dir) == 1 ? sz : 1))
 
@@ -1214,6 +1274,7 @@ static void remap_sweep(lo_state *s, int dir)
                                cv1[o + d1], cv1[o], cv1[o + 2 * d1], cvc1[o], cvc1[o + d1],
                                rv[o], rv[o + d1], dm[o], dir == 2);
         }
+        if (s->p.rke) rke_scatter(s, dir, u);
         LOOP3(ilo, nx, jlo, ny, klo, nz) { int64_t o = I3(ix, iy, iz); flux[o] *= dm[o]; }
         LOOP3(0, nx, 0, ny, 0, nz)
         {
@@ -1232,6 +1293,7 @@ static void eulerian_remap(lo_state *s)
 {
     DIMS(s);
     double *bx = s->f[SAMS_F_BX], *by = s->f[SAMS_F_BY], *bz = s->f[SAMS_F_BZ];
+    if (s->p.rke) memset(s->delta_ke, 0, (size_t)s->nbox * sizeof(double)); /* remap.cpp:38-41 */
     s->xpass = s->ypass = s->zpass = 1.0;
     LOOP3(-2, nx + 2, -1, ny + 2, -1, nz + 2) { int64_t o = I3(ix, iy, iz); bx[o] *= s->dxab[o]; }
     LOOP3(-1, nx + 2, -2, ny + 2, -1, nz + 2) { int64_t o = I3(ix, iy, iz); by[o] *= s->dyab[o]; }
@@ -1253,7 +1315,7 @@ static void eulerian_remap(lo_state *s)
 
 lo_state *lo_create(const sams_lare_params *p, const sams_lare_bcs *bcs)
 {
-    if (!p || !bcs || p->nx < 1 || p->ny < 1 || p->nz < 1 || p->geometry != 0 || p->rke) return NULL;
+    if (!p || !bcs || p->nx < 1 || p->ny < 1 || p->nz < 1 || p->geometry != 0) return NULL;
     lo_state *s = (lo_state *)calloc(1, sizeof(lo_state));
     if (!s) return NULL;
     s->p = *p;
@@ -1275,6 +1337,7 @@ lo_state *lo_create(const sams_lare_params *p, const sams_lare_bcs *bcs)
     ALLOC_BOX(bx1); ALLOC_BOX(by1); ALLOC_BOX(bz1); ALLOC_BOX(cv1); ALLOC_BOX(eta);
     ALLOC_BOX(flux_x); ALLOC_BOX(flux_y); ALLOC_BOX(flux_z); ALLOC_BOX(curlb); ALLOC_BOX(cs); ALLOC_BOX(cs_v);
     ALLOC_BOX(rho1); ALLOC_BOX(cv2); ALLOC_BOX(cvc1); ALLOC_BOX(db1); ALLOC_BOX(r_rho_v); ALLOC_BOX(rho_v1); ALLOC_BOX(flux);
+    ALLOC_BOX(delta_ke);
     build_grid(s);
     s->dt = 0.0; /* the runner's value-initialised data pack: dt = 0 before the first step */
     s->time = 0.0;
@@ -1294,7 +1357,8 @@ void lo_destroy(lo_state *s)
                       s->p_visc, s->visc_heat, s->alpha1, s->alpha2, s->alpha3, s->pressure, s->p_e, s->p_i,
                       s->rho_v, s->cv_v, s->fx, s->fy, s->fz, s->fx_visc, s->fy_visc, s->fz_visc,
                       s->bx1, s->by1, s->bz1, s->cv1, s->eta, s->flux_x, s->flux_y, s->flux_z, s->curlb,
-                      s->cs, s->cs_v, s->rho1, s->cv2, s->cvc1, s->db1, s->r_rho_v, s->rho_v1, s->flux};
+                      s->cs, s->cs_v, s->rho1, s->cv2, s->cvc1, s->db1, s->r_rho_v, s->rho_v1, s->flux,
+                      s->delta_ke};
     for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); ++i) free(arrs[i]);
     free(s);
 }
@@ -1356,6 +1420,7 @@ int lo_step_phase(lo_state *s, int phase)
     s->step++;
     s->time += s->dt;
     eulerian_remap(s);
+    if (s->p.rke) energy_correction(s);
     eta_calc(s);
     return 0;
 }

@@ -164,9 +164,12 @@ def field_slices(field, nx, ny, nz):
     return tuple(slice(0 if s else 1, n + 5) for s, n in zip(STAGGER[idx], (nx, ny, nz)))
 
 
-def run_reference(case, nx, ny, nz, steps, dump, seed=1, b0=0.0, ic=None, extra=(), binary=None):
-    """Run the reference harness binary; returns its JSON summary line."""
+def run_reference(case, nx, ny, nz, steps, dump, seed=1, b0=0.0, ic=None, extra=(), binary=None, threads=None):
+    """Run the reference harness binary; returns its JSON summary line.
+    threads=1 gives the reference's serial order of floating-point atomic
+    adds (the rke correction), i.e. a deterministic result."""
     import json
+    import os
     cmd = [binary or REF_BIN, "--case", case, "--nx", str(nx), "--ny", str(ny), "--nz", str(nz),
            "--steps", str(steps), "--seed", str(seed), "--quiet"]
     if b0:
@@ -176,5 +179,6 @@ def run_reference(case, nx, ny, nz, steps, dump, seed=1, b0=0.0, ic=None, extra=
     if ic:
         cmd += ["--ic", ic]
     cmd += list(extra)
-    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads)) if threads else None
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
     return json.loads(out.strip().splitlines()[-1])

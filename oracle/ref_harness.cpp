@@ -326,7 +326,7 @@ int main(int argc, char *argv[])
 {
     using namespace oracle;
     std::string dumpFinal;
-    bool quiet = false;
+    bool quiet = false, rke = false;
     for (int i = 1; i < argc; ++i)
     {
         std::string a = argv[i];
@@ -350,6 +350,7 @@ int main(int argc, char *argv[])
             g.dump_phase = p == "start" ? 0 : p == "half" ? 1 : 2;
         }
         else if (a == "--quiet") quiet = true;
+        else if (a == "--rke") rke = true;
         else { std::fprintf(stderr, "unknown argument %s\n", a.c_str()); return 2; }
     }
     if (g.case_id < 0 || sams_lare_case_setup(g.case_id, g.nx, g.ny, g.nz, g.b0, &g.params, &g.bcs) != 0)
@@ -357,6 +358,7 @@ int main(int argc, char *argv[])
         std::fprintf(stderr, "bad case/size\n");
         return 2;
     }
+    if (rke) g.params.rke = 1;  // remap kinetic-energy correction on
     if (g.dump_step >= 0) { g.dump_file = dumpFinal; dumpFinal.clear(); }
     if (quiet) std::cout.setstate(std::ios::failbit);
 

@@ -305,7 +305,7 @@ int Batch::set_stream(cudaStream_t s)
 long long Batch::bytes_for(const sams_lare_params &p)
 {
     Geom g = batch_geom(p);
-    return (long long)(SAMS_NFIELDS + NSCRATCH) * g.nelem * 8 + 8 * 2 * (p.nx + p.ny + p.nz + 18) + 256;
+    return (long long)(SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0)) * g.nelem * 8 + 8 * 2 * (p.nx + p.ny + p.nz + 18) + 256;
 }
 
 int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
@@ -315,7 +315,6 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
         return SAMS_ERR_INVALID;
     }
     if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
-    if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
     if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) { err = "empty domain"; return SAMS_ERR_INVALID; }
     {
         // tile planes and ghost shells are indexed with 32-bit integers
@@ -345,7 +344,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
         if (per && std::min(p.nx, std::min(p.ny, p.nz)) >= kBcSequentialBelow) s.periodic_groups |= 1u << f;
     }
     Geom g = batch_geom(p);
-    const size_t abytes = (size_t)(SAMS_NFIELDS + NSCRATCH) * (size_t)g.nelem * sizeof(double);
+    const size_t abytes = (size_t)(SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0)) * (size_t)g.nelem * sizeof(double);
     if ((rc = check(cudaMalloc(&s.arena, abytes), "cudaMalloc(solve)"))) return rc;
     cudaMemsetAsync(s.arena, 0, abytes, stream_);
     std::vector<double> dxb, dyb, dzb, dxc, dyc, dzc;
@@ -367,6 +366,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     c.g = g;
     for (int f = 0; f < SAMS_NFIELDS; ++f) c.f[f] = s.arena + (size_t)f * g.nelem;
     for (int q = 0; q < NSCRATCH; ++q) c.s[q] = s.arena + (size_t)(SAMS_NFIELDS + q) * g.nelem;
+    c.dke = p.rke ? s.arena + (size_t)(SAMS_NFIELDS + NSCRATCH) * g.nelem : nullptr;
     size_t o = 0;
     const double **slots[6] = {&c.ax.dxb, &c.ax.dyb, &c.ax.dzb, &c.ax.dxc, &c.ax.dyc, &c.ax.dzc};
     const size_t lens[6] = {dxb.size(), dyb.size(), dzb.size(), dxc.size(), dyc.size(), dzc.size()};
@@ -383,6 +383,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     c.p.eta0 = p.eta0;
     c.p.j_max = p.j_max;
     c.p.resistive = p.resistive_mhd ? 1 : 0;
+    c.p.rke = p.rke ? 1 : 0;
     c.sc = s.sc;
     s.bytes = (long long)abytes + (long long)(packed.size() * sizeof(double)) + (long long)sizeof(Scalars);
     s.live = true;
@@ -457,6 +458,7 @@ int Batch::rebuild()
     std::vector<Tile> tiles;
     long long shell = 0, slab[3] = {0, 0, 0};
     has_resistive_ = 0;
+    has_rke_ = 0;
     for (size_t q = 0; q < slots_.size(); ++q) {
         ctx[q] = slots_[q].ctx;
         bcs[q] = slots_[q].bc;
@@ -465,6 +467,7 @@ int Batch::rebuild()
         pf.push_back(slots_[q].periodic_groups);
         const Geom &g = slots_[q].ctx.g;
         has_resistive_ |= slots_[q].ctx.p.resistive;
+        has_rke_ |= slots_[q].ctx.p.rke;
         shell_off.push_back(shell);
         const long long e0 = g.nx + 5, e1 = g.ny + 5, e2 = g.nz + 5;
         shell += 5 * e1 * e2 + (long long)g.nx * 5 * e2 + (long long)g.nx * g.ny * 5;
@@ -602,6 +605,7 @@ void Batch::enqueue_step()
     launch<ops::Corr2>(0, false);
     bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY, false);
     // ---- remap ----
+    if (has_rke_) launch<ops::RkeZero>(0, false);
     launch<ops::BScale>(0, false);
     launch<ops::SweepVol<0>>(0, false);
     launch<ops::SweepCvc>(0, false);
@@ -611,6 +615,10 @@ void Batch::enqueue_step()
     bc_fill_dim(FM_DM, 0, false);
     launch<ops::SweepS6<0>>(0, false);
     launch<ops::SweepS7<0>>(0, false);
+    if (has_rke_) {  // solves without rke return at once (Phys::rke)
+        launch<ops::SweepRkeDk<0>>(0, false);
+        launch<ops::SweepRkeGather<0>>(0, false);
+    }
     launch<ops::SweepS8<0>>(0, false);
     bc_fill(FM_ALL9, false);
     launch<ops::SweepVol<1>>(0, false);
@@ -621,6 +629,10 @@ void Batch::enqueue_step()
     bc_fill_dim(FM_DM, 1, false);
     launch<ops::SweepS6<1>>(0, false);
     launch<ops::SweepS7<1>>(0, false);
+    if (has_rke_) {  // solves without rke return at once (Phys::rke)
+        launch<ops::SweepRkeDk<1>>(0, false);
+        launch<ops::SweepRkeGather<1>>(0, false);
+    }
     launch<ops::SweepS8<1>>(0, false);
     bc_fill(FM_ALL9, false);
     launch<ops::SweepVol<2>>(0, false);
@@ -631,10 +643,15 @@ void Batch::enqueue_step()
     bc_fill_dim(FM_DM, 2, false);
     launch<ops::SweepS6<2>>(0, false);
     launch<ops::SweepS7<2>>(0, false);
+    if (has_rke_) {  // solves without rke return at once (Phys::rke)
+        launch<ops::SweepRkeDk<2>>(0, false);
+        launch<ops::SweepRkeGather<2>>(0, false);
+    }
     launch<ops::SweepS8<2>>(0, false);
     bc_fill(FM_ALL9, false);
     launch<ops::BScale>(1, false);
     bc_fill(FM_BFIELD, false);
+    if (has_rke_) launch<ops::RkeEnergy>(0, false);
 }
 
 int Batch::step(long long nsteps)

@@ -99,6 +99,7 @@ private:
     long long shell_total_ = 0, slab_total_[3] = {0, 0, 0};
     int nlive_ = 0;
     int has_resistive_ = 0;
+    int has_rke_ = 0;
     size_t table_cap_bytes_ = 0;
     std::map<long long, cudaGraphExec_t> graphs_;
 };

@@ -54,6 +54,7 @@ struct Axes {
 struct Phys {
     double gamma, mu0, visc1, visc2_norm, dt_multiplier, eta_bg, eta0, j_max;
     int resistive;  // per-solve resistive flag (read by the batched launcher)
+    int rke;        // remap kinetic-energy correction on (Ctx::dke allocated)
 };
 
 // Per-solve device scalars.
@@ -108,6 +109,7 @@ struct Ctx {
     Phys p;
     double *f[13];
     double *s[NSCRATCH];
+    double *dke;  // delta_ke of the rke correction (null unless Phys::rke)
     Scalars *sc;
 };
 
@@ -216,12 +218,13 @@ __device__ __forceinline__ double energy_flux(double v_advect, double dt, double
     return (fu + Di * (1.0 - dmu)) * dm;
 }
 
-// Momentum flux times dm (x_mom_flux xremap.cpp:485-566 and analogues;
-// the z sweep divides |dm| by (dzbu * rhou) in one step, zremap.cpp:509).
+// Momentum flux before its product with dm (x_mom_flux xremap.cpp:485-566
+// and analogues; the z sweep divides |dm| by (dzbu * rhou) in one step,
+// zremap.cpp:509).
 template <bool ZFORM>
-__device__ __forceinline__ double mom_flux_dm(double v_advect, double dt, double area, double fm, double fi,
-                                              double fp, double fp2, double dci, double dcm, double dcp,
-                                              double cvci, double cvcp, double rvi, double rvp, double dm)
+__device__ __forceinline__ double mom_flux(double v_advect, double dt, double area, double fm, double fi,
+                                           double fp, double fp2, double dci, double dcm, double dcp,
+                                           double cvci, double cvcp, double rvi, double rvp, double dm)
 {
     double o_v = v_advect * dt * area;
     double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
@@ -236,8 +239,7 @@ __device__ __forceinline__ double mom_flux_dm(double v_advect, double dt, double
     double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
     double rhou = rvi * vad_p + rvp * vad_m;
     double dmu = ZFORM ? fabs(dm) / (dxbu * rhou) : fabs(dm) / dxbu / rhou;
-    double flux = fu + Di * (1.0 - dmu);
-    return flux * dm;
+    return fu + Di * (1.0 - dmu);
 }
 
 // Caramana edge viscosity (lagran.cpp:56-93).  v[a] are the four points

@@ -87,8 +87,11 @@ __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int
 // Lagrangian phase
 // ---------------------------------------------------------------------------
 
-// Sound speed on cells; with resistive MHD also keeps p_e, which the
-// predictor needs from before the Ohmic heating (lagran.cpp:121, 606).
+// Sound speed on cells; with resistive MHD also keeps p_e and p_i, which the
+// predictor reads as they were at the start of the step (lagran.cpp:121-123,
+// 606-607): between the two, the resistive sub-steps heat the electrons and
+// refill the energies' ghost cells (energy_bcs), so recomputing them there
+// would differ wherever a ghost was not already its boundary value.
 struct CellPrep {
     static constexpr int kMinBlocks = 6;  // blocks of 256 per SM (register cap), tuned on B200
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
@@ -111,7 +114,10 @@ struct CellPrep {
         double rmin = pmax(rho, NONE_ZERO);
         double b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
         c.s[S_CS][o] = sqrt((gm * p + b2) / rmin);
-        if (resistive) c.s[S_PE][o] = pe;
+        if (resistive) {
+            c.s[S_PE][o] = pe;
+            c.s[S_PI][o] = pi;
+        }
     }
 };
 
@@ -453,7 +459,7 @@ struct Pred1 {
         double rho = __ldg(c.f[SAMS_F_RHO] + o), ee = __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
         double ei = __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double pe = resistive ? c.s[S_PE][o] : (gm - 1.0) * rho * ee;
-        double pi = (gm - 1.0) * rho * ei;
+        double pi = resistive ? c.s[S_PI][o] : (gm - 1.0) * rho * ei;
         double dvv = cv1 / vol - 1.0;
         double e1_e = ee - pe * dvv / rho;
         double e1_i = ei - pi * dvv / rho;
@@ -976,12 +982,18 @@ struct SweepS7 {
         const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
         const double rvi = rv[o], rvp = rv[o + d];
         const RO ux{c.f[SAMS_F_VX]}, uy{c.f[SAMS_F_VY]}, uz{c.f[SAMS_F_VZ]};
-        c.s[S_R_FM1][o] = mom_flux_dm<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
-                                                cvi, cvp, rvi, rvp, dmv);
-        c.s[S_R_FM2][o] = mom_flux_dm<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
-                                                cvi, cvp, rvi, rvp, dmv);
-        c.s[S_R_FM3][o] = mom_flux_dm<DIR == 2>(v, dt, area, uz[o - d], uz[o], uz[o + d], uz[o + 2 * d], dci, dcm, dcp,
-                                                cvi, cvp, rvi, rvp, dmv);
+        const double f1 = mom_flux<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        const double f2 = mom_flux<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        const double f3 = mom_flux<DIR == 2>(v, dt, area, uz[o - d], uz[o], uz[o + d], uz[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        // with the rke correction the flux is kept as is (its kinetic-energy
+        // error needs it) and SweepS8 takes the product with dm
+        const bool raw = c.p.rke != 0;
+        c.s[S_R_FM1][o] = raw ? f1 : f1 * dmv;
+        c.s[S_R_FM2][o] = raw ? f2 : f2 * dmv;
+        c.s[S_R_FM3][o] = raw ? f3 : f3 * dmv;
     }
 };
 
@@ -1005,9 +1017,136 @@ struct SweepS8 {
         const double den = cv2o * rho_v1;
         double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
         const RO f1{c.s[S_R_FM1]}, f2{c.s[S_R_FM2]}, f3{c.s[S_R_FM3]};
+        if (c.p.rke) {  // raw fluxes: the reference's flux *= dm, then the update
+            const double dm0 = dmn[o - d], dm1 = dmn[o];
+            ux[o] = (rvo * ux[o] * cvco + f1[o - d] * dm0 - f1[o] * dm1) / den;
+            uy[o] = (rvo * uy[o] * cvco + f2[o - d] * dm0 - f2[o] * dm1) / den;
+            uz[o] = (rvo * uz[o] * cvco + f3[o - d] * dm0 - f3[o] * dm1) / den;
+            return;
+        }
         ux[o] = (rvo * ux[o] * cvco + f1[o - d] - f1[o]) / den;
         uy[o] = (rvo * uy[o] * cvco + f2[o - d] - f2[o]) / den;
         uz[o] = (rvo * uz[o] * cvco + f3[o - d] - f3[o]) / den;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Remap kinetic-energy correction (rke; Phys::rke, Ctx::dke)
+// ---------------------------------------------------------------------------
+
+// delta_ke = 0 before the sweeps (remap.cpp:38-41).
+struct RkeZero {
+    static constexpr int kMinBlocks = 6;
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        if (c.p.rke) c.dke[box_off(c.g, i, j, k)] = 0.0;
+    }
+};
+
+// Kinetic-energy error of the sweep's three momentum fluxes at each face,
+// the dk of x_mom_flux (xremap.cpp:534-558) and its y/z analogues
+// (yremap.cpp:557-583, zremap.cpp:513-536), one per velocity component into
+// S_FX/S_FY/S_FZ.  Reads the raw fluxes of SweepS7 and the velocities before
+// SweepS8 updates them; the post-sweep vertex density is formed as in S8.
+template <int DIR>
+struct SweepRkeDk {
+    static constexpr int kMinBlocks = 4;
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 0, DIR == 0 ? g.nx - 1 : g.nx, 0, DIR == 1 ? g.ny - 1 : g.ny, 0,
+                   DIR == 2 ? g.nz - 1 : g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        if (!c.p.rke) return;
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
+        const int op = o + d, om = o - d;
+        const RO rv{c.s[S_R_RVN]}, cvc1{c.s[S_R_CVC1]}, cv2n{c.s[S_R_CV2N]}, dmn{c.s[S_R_DMN]};
+        const double rv1o = (rv[o] * cvc1[o] + dmn[om] - dmn[o]) / cv2n[o];
+        const double rv1p = (rv[op] * cvc1[op] + dmn[o] - dmn[op]) / cv2n[op];
+        const double m = rv1o * cv2n[o];
+        const double mp = rv1p * cv2n[op];
+        const double dmm = dmn[om], dm0 = dmn[o], dmp = dmn[op];
+        const int fluxes[3] = {S_R_FM1, S_R_FM2, S_R_FM3};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const RO u{c.f[SAMS_F_VX + q]}, fl{c.s[fluxes[q]]};
+            const double uo = u[o], up = u[op], flm = fl[om], fl0 = fl[o], flp = fl[op];
+            const double ai = (uo - flm) * dmm / m - (uo - fl0) * dm0 / m;
+            const double aip = (up - fl0) * dm0 / mp - (up - flp) * dmp / mp;
+            double dk = (up - uo) * (fl0 - 0.5 * (up + uo)) - 0.5 * ai * (uo - fl0) + 0.5 * aip * (up - fl0);
+            dk = dk * dm0 * 0.5;
+            c.s[S_FX + q][o] = dk;
+        }
+    }
+};
+
+// delta_ke gathers the dk of the four faces around each node, for vx, vy and
+// vz in turn, adding in the order the reference's loops add them serially
+// (source faces in index order).  The reference adds with atomics from
+// parallel loops, so its own result is this one only when run on one thread.
+template <int DIR>
+struct SweepRkeGather {
+    static constexpr int kMinBlocks = 6;
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, DIR == 0 ? 1 : 0, DIR == 0 ? g.nx : g.nx + 1, DIR == 1 ? 1 : 0,
+                   DIR == 1 ? g.ny : g.ny + 1, DIR == 2 ? 1 : 0, DIR == 2 ? g.nz : g.nz + 1);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        if (!c.p.rke) return;
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        // the two transverse dimensions, lower index first, and their extents
+        const int t1 = DIR == 0 ? 1 : 0, t2 = DIR == 2 ? 1 : 2;
+        const int q[3] = {i, j, k};
+        const int n[3] = {g.nx, g.ny, g.nz};
+        const int st[3] = {g.sx, g.sy, 1};
+        const int src0 = o - st[DIR];
+        double acc = c.dke[o];
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+            const RO dk{c.s[S_FX + comp]};
+#pragma unroll
+            for (int a = -1; a <= 0; ++a) {
+                const int qa = q[t1] + a;
+                if (qa < 0 || qa > n[t1]) continue;
+#pragma unroll
+                for (int b = -1; b <= 0; ++b) {
+                    const int qb = q[t2] + b;
+                    if (qb < 0 || qb > n[t2]) continue;
+                    acc += dk[src0 + a * st[t1] + b * st[t2]];
+                }
+            }
+        }
+        c.dke[o] = acc;
+    }
+};
+
+// energy_correction (diagnostics.cpp:125-135) after the remap's last
+// boundary fill; the energies' ghosts are left as that fill set them.
+struct RkeEnergy {
+    static constexpr int kMinBlocks = 6;
+    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    {
+        set_bounds(lo, hi, 1, g.nx, 1, g.ny, 1, g.nz);
+    }
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        if (!c.p.rke) return;
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        const double d = pmax(-c.dke[o], 0.0) / (__ldg(c.f[SAMS_F_RHO] + o) * cv_at(c, i, j, k));
+        double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+        ee[o] += 0.5 * d;
+        ei[o] += 0.5 * d;
     }
 };
 

@@ -255,7 +255,6 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     if (p.nx < 1 || p.ny < 1 || p.nz < 1) { err = "grid sizes must be >= 1"; return SAMS_ERR_INVALID; }
     if (p.nx > 60000 || p.ny > 60000 || p.nz > 60000) { err = "grid size too large"; return SAMS_ERR_INVALID; }
     if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
-    if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
     if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) {
         err = "empty domain";
         return SAMS_ERR_INVALID;
@@ -291,12 +290,14 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     g.sy = (int)zrow;
     g.sx = (int)sx;
     g.nelem = (long long)(p.nx + 5) * sx;
-    const long long narr = SAMS_NFIELDS + NSCRATCH;
+    // the rke correction keeps one more array (delta_ke) across the sweeps
+    const long long narr = SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0);
     const size_t abytes = (size_t)narr * (size_t)g.nelem * sizeof(double);
     if ((rc = check(cudaMalloc(&arena_, abytes), "cudaMalloc(state)"))) return rc;
     if ((rc = check(cudaMemsetAsync(arena_, 0, abytes, stream_), "cudaMemset(state)"))) return rc;
     for (int f = 0; f < SAMS_NFIELDS; ++f) ctx_.f[f] = arena_ + (size_t)f * g.nelem;
     for (int s = 0; s < NSCRATCH; ++s) ctx_.s[s] = arena_ + (size_t)(SAMS_NFIELDS + s) * g.nelem;
+    ctx_.dke = p.rke ? arena_ + (size_t)(SAMS_NFIELDS + NSCRATCH) * g.nelem : nullptr;
 
     // 1-D spacings: dxb, dyb, dzb, dxc, dyc, dzc, each (n + 6) long.
     std::vector<double> dxb, dyb, dzb, dxc, dyc, dzc;
@@ -324,6 +325,7 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     ctx_.p.eta0 = p.eta0;
     ctx_.p.j_max = p.j_max;
     ctx_.p.resistive = p.resistive_mhd ? 1 : 0;
+    ctx_.p.rke = p.rke ? 1 : 0;
 
     if ((rc = check(cudaMalloc(&sc_, sizeof(Scalars)), "cudaMalloc(scalars)"))) return rc;
     Scalars s0{};
@@ -339,7 +341,10 @@ int Solver::init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, c
                           cudaStream_t stream)
 {
     if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
-    if (p.rke != 0) { err = "the remap kinetic-energy correction (rke) is not built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.rke != 0) {
+        err = "the remap kinetic-energy correction (rke) needs an array this entry point does not have";
+        return SAMS_ERR_UNSUPPORTED;
+    }
     p_ = p;
     device_ = device;
     for (int f = 0; f < SAMS_NFIELDS; ++f)
@@ -537,6 +542,7 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY);
     mark(2);
     // ---- remap ----
+    if (p_.rke) launch<ops::RkeZero>(0);
     launch<ops::BScale>(0);
     launch<ops::SweepVol<0>>(0);
     launch<ops::SweepCvc>(0);
@@ -546,6 +552,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     bc_fill_dim(FM_DM, 0);
     launch<ops::SweepS6<0>>(0);
     launch<ops::SweepS7<0>>(0);
+    if (p_.rke) {
+        launch<ops::SweepRkeDk<0>>(0);
+        launch<ops::SweepRkeGather<0>>(0);
+    }
     launch<ops::SweepS8<0>>(0);
     bc_fill(FM_ALL9);
     mark(3);
@@ -557,6 +567,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     bc_fill_dim(FM_DM, 1);
     launch<ops::SweepS6<1>>(0);
     launch<ops::SweepS7<1>>(0);
+    if (p_.rke) {
+        launch<ops::SweepRkeDk<1>>(0);
+        launch<ops::SweepRkeGather<1>>(0);
+    }
     launch<ops::SweepS8<1>>(0);
     bc_fill(FM_ALL9);
     mark(4);
@@ -568,10 +582,15 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     bc_fill_dim(FM_DM, 2);
     launch<ops::SweepS6<2>>(0);
     launch<ops::SweepS7<2>>(0);
+    if (p_.rke) {
+        launch<ops::SweepRkeDk<2>>(0);
+        launch<ops::SweepRkeGather<2>>(0);
+    }
     launch<ops::SweepS8<2>>(0);
     bc_fill(FM_ALL9);
     launch<ops::BScale>(1);
     bc_fill(FM_BFIELD);
+    if (p_.rke) launch<ops::RkeEnergy>(0);  // after the remap (shared_data.h:414-417)
     mark(5);
 }
 

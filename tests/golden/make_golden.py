@@ -23,7 +23,7 @@ from oracle import lare_oracle as lo  # noqa: E402
 from oracle import dumpio  # noqa: E402
 from oracle.dumpio import Dump  # noqa: E402
 
-# (name, case, nx, ny, nz, steps, seed, b0)
+# (name, case, nx, ny, nz, steps, seed, b0[, rke])
 CASES = [
     ("ot_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0),
     ("ot_7x5x3_s3", "ot", 7, 5, 3, 3, 1, 0.0),
@@ -35,6 +35,10 @@ CASES = [
     ("ot_12x10x2_s4", "ot", 12, 10, 2, 4, 1, 0.0),
     ("ot_8x6x1_s3", "ot", 8, 6, 1, 3, 1, 0.0),
     ("harris_10x2x4_s3", "harris", 10, 2, 4, 3, 3, 0.0),
+    # the remap kinetic-energy correction on (rke): the reference run on one
+    # thread, where its atomic adds happen in loop order
+    ("ot_rke_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0, 1),
+    ("rf_rke_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0, 1),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 # (file, case, nx, ny, nz, steps, seed): the reference's full harness state
@@ -48,16 +52,18 @@ def main():
     lo.build()
     if not os.path.exists(lo.REF_BIN):
         raise SystemExit("reference harness not built (needs the reference tree)")
-    for name, case, nx, ny, nz, steps, seed, b0 in CASES:
+    for name, case, nx, ny, nz, steps, seed, b0, *opt in CASES:
+        rke = opt[0] if opt else 0
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "d.dump")
-            summary = lo.run_reference(case, nx, ny, nz, steps, path, seed=seed, b0=b0)
+            summary = lo.run_reference(case, nx, ny, nz, steps, path, seed=seed, b0=b0,
+                                       extra=["--rke"] if rke else (), threads=1 if rke else None)
             d = Dump(path)
             out = {}
             for f in STATE:
                 out[f] = d.box(f)
             out["dts"] = np.array(d.header["dts"])
-            meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0,
+            meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0, rke=rke,
                         time=summary["time"], generator="oracle/_ref/lare_ref (reference LARE3D)")
             out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)

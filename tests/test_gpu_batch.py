@@ -14,8 +14,9 @@ MIX = [("ot", (16, 12, 4), 1, 0.0), ("ot", (24, 24, 4), 2, 0.9 / (4 * np.pi) ** 
        ("ot", (20, 16, 2), 6, 0.0), ("rf", (10, 2, 8), 7, 0.0)]
 
 
-def _solo(case, n, seed, b0, steps):
+def _solo(case, n, seed, b0, steps, rke=0):
     p, b = lare.case_setup(case, *n, b0)
+    p.rke = rke
     s = lare.LARE3D(p, b)
     s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
     s.step(steps)
@@ -25,8 +26,9 @@ def _solo(case, n, seed, b0, steps):
     return out, st
 
 
-def _add(batch, case, n, seed, b0):
+def _add(batch, case, n, seed, b0, rke=0):
     p, b = lare.case_setup(case, *n, b0)
+    p.rke = rke
     return batch.add(p, b, lare.case_fields(case, p, seed=seed, b0=b0))
 
 
@@ -72,4 +74,20 @@ def test_batch_add_remove_midrun_and_autotune_restores():
     _check_equal(bt, b, MIX[2][0], MIX[2][1], ref_b, st_b)
     ref_c, st_c = _solo(*MIX[3], steps=4)
     _check_equal(bt, c, MIX[3][0], MIX[3][1], ref_c, st_c)
+    bt.close()
+
+
+def test_batch_mixing_rke_and_plain_solves_equals_solo():
+    """Solves with and without the remap kinetic-energy correction share a
+    batch: the correction's launches run for the batch and leave the others'
+    state alone."""
+    mix = [("rf", (12, 12, 12), 3, 0.0, 1), ("ot", (24, 24, 4), 2, 0.0, 0), ("harris", (16, 12, 6), 4, 0.0, 1),
+           ("ot", (20, 16, 2), 6, 0.0, 1)]
+    bt = lare.Batch()
+    ids = [_add(bt, *m) for m in mix]
+    bt.step(5, graph=True)
+    bt.synchronize()
+    for sid, (case, n, seed, b0, rke) in zip(ids, mix):
+        ref, st = _solo(case, n, seed, b0, 5, rke)
+        _check_equal(bt, sid, case, n, ref, st)
     bt.close()

@@ -14,8 +14,9 @@ from oracle import lare_oracle as lo
 from tests.golden.make_golden import CASES, STATE, load
 
 
-def _run_checker(case, nx, ny, nz, steps, seed, b0):
+def _run_checker(case, nx, ny, nz, steps, seed, b0, rke=0):
     p, b = lo.case_setup(case, nx, ny, nz, b0)
+    p.rke = rke
     o = lo.Oracle(p, b, lo.case_fields(case, p, seed=seed, b0=b0))
     dts = []
     for _ in range(steps):
@@ -27,7 +28,8 @@ def _run_checker(case, nx, ny, nz, steps, seed, b0):
 @pytest.mark.parametrize("name", [c[0] for c in CASES])
 def test_checker_matches_reference_golden(name, oracle_lib):
     z, meta = load(name)
-    o, dts = _run_checker(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["steps"], meta["seed"], meta["b0"])
+    o, dts = _run_checker(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["steps"], meta["seed"], meta["b0"],
+                          meta.get("rke", 0))
     assert np.array_equal(np.array(dts), z["dts"]), "dt history differs"
     for f in STATE:
         ref = z[f]
@@ -37,15 +39,19 @@ def test_checker_matches_reference_golden(name, oracle_lib):
 
 
 @pytest.mark.skipif(not os.path.exists(lo.REF_BIN), reason="reference harness binary not built here")
-@pytest.mark.parametrize("case,n,steps", [("ot", (9, 11, 5), 12), ("rf", (8, 8, 8), 6), ("harris", (10, 8, 4), 6),
-                                          ("rf", (8, 8, 2), 3), ("ot", (2, 9, 5), 3)])
-def test_checker_matches_reference_binary(case, n, steps, tmp_path, oracle_lib):
+@pytest.mark.parametrize("case,n,steps,rke", [("ot", (9, 11, 5), 12, 0), ("rf", (8, 8, 8), 6, 0),
+                                              ("harris", (10, 8, 4), 6, 0), ("rf", (8, 8, 2), 3, 0),
+                                              ("ot", (2, 9, 5), 3, 0), ("ot", (9, 11, 5), 6, 1),
+                                              ("harris", (10, 8, 4), 4, 1)])
+def test_checker_matches_reference_binary(case, n, steps, rke, tmp_path, oracle_lib):
+    """rke = 1: the reference on one thread (its atomic adds in loop order)."""
     from oracle.dumpio import Dump
     nx, ny, nz = n
     dump = str(tmp_path / "ref.dump")
-    lo.run_reference(case, nx, ny, nz, steps, dump, seed=11)
+    lo.run_reference(case, nx, ny, nz, steps, dump, seed=11, extra=["--rke"] if rke else (),
+                     threads=1 if rke else None)
     d = Dump(dump)
-    o, dts = _run_checker(case, nx, ny, nz, steps, 11, 0.0)
+    o, dts = _run_checker(case, nx, ny, nz, steps, 11, 0.0, rke)
     assert dts == d.header["dts"]
     for f in lo.FIELD_NAMES:
         ref = d.box(f)
@@ -80,3 +86,36 @@ def test_periodic_mass_conservation_checker(oracle_lib):
     o.step(20)
     m1 = (o.field("rho")[3:-2, 3:-2, 3:-2] * cv).sum()
     assert abs(m1 - m0) / m0 < 1e-13
+
+
+@pytest.mark.skipif(not os.path.exists(lo.REF_BIN), reason="reference harness binary not built here")
+def test_checker_matches_reference_with_inconsistent_ghosts(tmp_path, oracle_lib):
+    """Initial energies whose ghost cells are not their boundary values (an IC
+    package may fill ghosts analytically): in a resistive run the predictor
+    must use the pressures of the step's start, before the sub-steps refill
+    the energies' ghosts."""
+    from oracle.dumpio import Dump
+    n = (10, 8, 6)
+    p, b = lo.case_setup("rf", *n)
+    fields = lo.case_fields("rf", p, seed=3)
+    for f in (1, 2):  # e_e, e_i: ghosts scaled, interior untouched
+        inner = fields[f][3:-2, 3:-2, 3:-2].copy()
+        fields[f] *= 1.25
+        fields[f][3:-2, 3:-2, 3:-2] = inner
+    ic = tmp_path / "ic.bin"
+    with open(ic, "wb") as fh:
+        for a in fields:
+            fh.write(np.ascontiguousarray(a).tobytes())
+    dump = str(tmp_path / "ref.dump")
+    lo.run_reference("rf", *n, 3, dump, ic=str(ic))
+    d = Dump(dump)
+    o = lo.Oracle(p, b, fields)
+    dts = []
+    for _ in range(3):
+        o.step(1)
+        dts.append(o.dt)
+    assert dts == d.header["dts"]
+    for f in lo.FIELD_NAMES:
+        ref = d.box(f)
+        m = ~np.isnan(ref)
+        assert np.array_equal(o.field(f)[m], ref[m]), f
