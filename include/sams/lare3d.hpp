@@ -19,9 +19,8 @@
 // The solver is created at the first startOfTimestep, after the IC package
 // has written the harness variables and attached its boundary conditions;
 // from then on the state lives on the GPU and syncToHost() refreshes the host
-// copy.  Supported: Cartesian geometry, with or without the remap
-// kinetic-energy correction (rke); other geometries fail with
-// std::runtime_error at that first step.
+// copy.  Cartesian, cylindrical and spherical geometry, with or without the
+// remap kinetic-energy correction (rke).
 #pragma once
 
 #include <cstring>

@@ -51,7 +51,8 @@ const char *sams_lare_last_error(void);
  * (include/runner/runner.h:456-464).  Boundary conditions are copied; they
  * replace the IC package's setBoundaryConditions
  * (variableDef::addBoundaryCondition, include/harness/variableDef.h:402-481).
- * Supported: Cartesian geometry (rke on or off). */
+ * Supported: Cartesian, cylindrical and spherical geometry (params.geometry
+ * 0, 1, 2), rke on or off. */
 int sams_lare_create(const sams_lare_params *params, const sams_lare_bcs *bcs,
                      int device, sams_lare_solver **out);
 

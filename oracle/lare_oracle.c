@@ -8,11 +8,12 @@
  * Reference locations are cited per function (paths relative to the
  * reference project root).
  *
- * Geometry: Cartesian only.  All metric factors hy, hyc, hz, hzc, hz1, hz2
- * are 1.0 there (setup.cpp:277-304) and multiplying or dividing by 1.0 is
- * exact, so they are dropped.  The Lagrangian position arrays x, y, z are
- * diagnostics in Cartesian geometry (never read by the physics) and are not
- * kept.  The second rkstep of resistive_effects (lagran.cpp:504) writes only
+ * Geometry: Cartesian, cylindrical and spherical.  The metric factors hy,
+ * hyc, hyv (per x) and hz, hz1, hz2, hzc (per x and y) are built as
+ * LARE3D::grid builds them (setup.cpp:260-335); in Cartesian geometry they
+ * are 1.0 and multiplying or dividing by them changes nothing.  The
+ * Lagrangian position arrays x, y, z are diagnostics (never read by the
+ * physics) and are not kept.  The second rkstep of resistive_effects (lagran.cpp:504) writes only
  * flux_x/y/z and curlb, which nothing reads before they are recomputed, so it
  * is not repeated.
  */
@@ -40,6 +41,8 @@ struct lo_state {
     /* remap temporaries (remapData.h:23-32) */
     double *rho1, *cv2, *cvc1, *db1, *r_rho_v, *rho_v1, *flux;
     double *delta_ke; /* remap kinetic-energy correction (rke only, setup.cpp:251) */
+    /* geometry factors (setup.cpp:277-335): per x at [x + 2], per (x, y) at H2 */
+    double *hy, *hyc, *hyv, *hz, *hz1, *hz2, *hzc, *cot_yb;
     double dt, dtr, time, visc2_norm;
     int64_t step;
     double xpass, ypass, zpass;
@@ -51,6 +54,7 @@ struct lo_state {
     (void)nx; (void)ny; (void)nz; (void)sy; (void)sz
 #define I3(i, j, k) ((((int64_t)(i) + 2) * sy + ((int64_t)(j) + 2)) * sz + ((int64_t)(k) + 2))
 #define A1(i) ((int64_t)(i) + 2)
+#define H2(i, j) (((int64_t)(i) + 2) * sy + ((int64_t)(j) + 2))
 
 #define LOOP3(ilo, ihi, jlo, jhi, klo, khi)                        \
     _Pragma("omp parallel for schedule(static)")                   \
@@ -193,34 +197,75 @@ static void build_grid(lo_state *s)
     build_axis(s->p.x_min, s->p.x_max, nx, s->xb, s->xc, s->dxb, s->dxc);
     build_axis(s->p.y_min, s->p.y_max, ny, s->yb, s->yc, s->dyb, s->dyc);
     build_axis(s->p.z_min, s->p.z_max, nz, s->zb, s->zc, s->dzb, s->dzc);
-    const double *dxb = s->dxb, *dyb = s->dyb, *dzb = s->dzb, *dzc = s->dzc;
+    const double *dxb = s->dxb, *dyb = s->dyb, *dzb = s->dzb, *dzc = s->dzc, *dyc = s->dyc;
+    double *hy = s->hy, *hyc = s->hyc, *hyv = s->hyv, *hz = s->hz, *hz1 = s->hz1, *hz2 = s->hz2, *hzc = s->hzc;
+    const int geo = s->p.geometry;
+    /* setup.cpp:277-292; LARE::none_zero = DBL_MIN (constants.h:43) */
+    for (int64_t ix = -2; ix <= nx + 2; ++ix) {
+        if (geo == 0) {
+            hy[A1(ix)] = hyc[A1(ix)] = hyv[A1(ix)] = 1.0;
+        } else {
+            hy[A1(ix)] = fabs(s->xb[A1(ix)]);
+            hyc[A1(ix)] = fabs(s->xc[A1(ix)]);
+            hyv[A1(ix)] = (fabs(s->xc[A1(0)]) < DBL_MIN && ix == 1) ? fabs(s->xc[A1(ix)]) : 0.25 * fabs(s->xc[A1(ix)]);
+        }
+    }
+    /* setup.cpp:294-334 */
+    for (int64_t ix = -2; ix <= nx + 2; ++ix)
+        for (int64_t iy = -2; iy <= ny + 2; ++iy)
+            hz[H2(ix, iy)] = hz1[H2(ix, iy)] = hz2[H2(ix, iy)] = hzc[H2(ix, iy)] = 1.0;
+    if (geo == 2) {
+        for (int64_t iy = -2; iy <= ny + 2; ++iy) {
+            double sn = fabs(sin(s->yb[A1(iy)]));
+            hz[H2(-2, iy)] = hy[A1(-2)] * sn;
+            for (int64_t ix = -1; ix <= nx + 2; ++ix) {
+                hz[H2(ix, iy)] = hy[A1(ix)] * sn;
+                hz2[H2(ix, iy)] = hyc[A1(ix)] * sn;
+            }
+        }
+        for (int64_t iy = -1; iy <= ny + 2; ++iy) {
+            double sc = fabs(sin(s->yc[A1(iy)]));
+            hz1[H2(-2, iy)] = hy[A1(-2)] * sc;
+            for (int64_t ix = -1; ix <= nx + 2; ++ix) {
+                hz1[H2(ix, iy)] = hy[A1(ix)] * sc;
+                hzc[H2(ix, iy)] = hyc[A1(ix)] * sc;
+            }
+        }
+    }
+    /* 1/tan(yb) of the spherical force terms (lagran.cpp:713) */
+    for (int64_t iy = -2; iy <= ny + 2; ++iy) s->cot_yb[A1(iy)] = geo == 2 ? 1.0 / tan(s->yb[A1(iy)]) : 0.0;
+    /* cell-centred areas and volumes (setup.cpp:337-354) */
     for (int64_t iy = -1; iy <= ny + 2; ++iy)
         for (int64_t iz = -1; iz <= nz + 2; ++iz) {
             double dy = dyb[A1(iy)], dz = dzb[A1(iz)], dydz = dy * dz;
-            s->dxab[I3(-2, iy, iz)] = dydz;
+            s->dxab[I3(-2, iy, iz)] = dydz * hy[A1(-2)] * hz1[H2(-2, iy)];
             for (int64_t ix = -1; ix <= nx + 2; ++ix) {
                 double dx = dxb[A1(ix)];
-                s->dxab[I3(ix, iy, iz)] = dydz;
-                s->dyab[I3(ix, iy, iz)] = dx * dz;
-                s->dzab[I3(ix, iy, iz)] = dx * dy;
-                s->cv[I3(ix, iy, iz)] = dx * dydz;
+                s->dxab[I3(ix, iy, iz)] = dydz * hy[A1(ix)] * hz1[H2(ix, iy)];
+                s->dyab[I3(ix, iy, iz)] = dx * dz * hz2[H2(ix, iy)];
+                s->dzab[I3(ix, iy, iz)] = dx * dy * hy[A1(ix)];
+                s->cv[I3(ix, iy, iz)] = dx * dydz * hyc[A1(ix)] * hzc[H2(ix, iy)];
             }
         }
+    /* negative y and z boundaries (setup.cpp:356-374; the dzab(-2) pass with
+     * dyc is overwritten by the one with dyb) */
     for (int64_t ix = -1; ix <= nx + 2; ++ix)
         for (int64_t iz = -1; iz <= nz + 2; ++iz)
-            s->dyab[I3(ix, -2, iz)] = dxb[A1(ix)] * dzb[A1(iz)];
+            s->dyab[I3(ix, -2, iz)] = dxb[A1(ix)] * dzb[A1(iz)] * hz2[H2(ix, -2)];
+    (void)dyc;
     for (int64_t ix = -1; ix <= nx + 2; ++ix)
         for (int64_t iy = -1; iy <= ny + 2; ++iy)
-            s->dzab[I3(ix, iy, -2)] = dxb[A1(ix)] * dyb[A1(iy)];
+            s->dzab[I3(ix, iy, -2)] = dxb[A1(ix)] * dyb[A1(iy)] * hyc[A1(ix)];
+    /* node-centred areas and volumes (setup.cpp:375-390) */
     for (int64_t ix = -1; ix <= nx + 2; ++ix)
         for (int64_t iy = -1; iy <= ny + 2; ++iy)
             for (int64_t iz = -1; iz <= nz + 2; ++iz) {
                 double dx = dxb[A1(ix)], dy = dyb[A1(iy)], dz = dzc[A1(iz)];
                 double dydz = dy * dz;
-                s->dxac[I3(ix, iy, iz)] = dydz;
-                s->dyac[I3(ix, iy, iz)] = dx * dz;
-                s->dzac[I3(ix, iy, iz)] = dx * dy;
-                s->cvc[I3(ix, iy, iz)] = dx * dydz;
+                s->dxac[I3(ix, iy, iz)] = dydz * hyc[A1(ix)] * hz2[H2(ix, iy)];
+                s->dyac[I3(ix, iy, iz)] = dx * dz * hz1[H2(ix, iy)];
+                s->dzac[I3(ix, iy, iz)] = dx * dy * hy[A1(ix)];
+                s->cvc[I3(ix, iy, iz)] = dx * dydz * hyv[A1(ix)] * hz[H2(ix, iy)];
             }
 }
 
@@ -315,7 +360,8 @@ static void shock_viscosity(lo_state *s)
     {
         int64_t o1 = I3(ix, iy - 1, iz - 1), o2 = I3(ix, iy, iz - 1);
         int64_t o0 = I3(ix, iy - 2, iz - 1), o3 = I3(ix, iy + 1, iz - 1);
-        double dx = dyb[A1(iy)], dxp = dyb[A1(iy + 1)], dxm = dyb[A1(iy - 1)];
+        const double h = s->hy[A1(ix)];
+        double dx = dyb[A1(iy)] * h, dxp = dyb[A1(iy + 1)] * h, dxm = dyb[A1(iy - 1)] * h;
         double dvdots = -(vy[o1] - vy[o2]);
         double cs_edge = pmin(cs_v[o1], cs_v[o2]);
         a2a[I3(ix, iy, iz)] = edge_viscosity(s, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
@@ -325,7 +371,8 @@ static void shock_viscosity(lo_state *s)
     {
         int64_t o1 = I3(ix, iy, iz - 1), o2 = I3(ix, iy, iz);
         int64_t o0 = I3(ix, iy, iz - 2), o3 = I3(ix, iy, iz + 1);
-        double dx = dzb[A1(iz)], dxp = dzb[A1(iz + 1)], dxm = dzb[A1(iz - 1)];
+        const double h = s->hz[H2(ix, iy)];
+        double dx = dzb[A1(iz)] * h, dxp = dzb[A1(iz + 1)] * h, dxm = dzb[A1(iz - 1)] * h;
         double dvdots = -(vz[o1] - vz[o2]);
         double cs_edge = pmin(cs_v[o1], cs_v[o2]);
         a3a[I3(ix, iy, iz)] = edge_viscosity(s, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
@@ -353,7 +400,7 @@ static void shock_viscosity(lo_state *s)
         p_visc[o] = pmax(p_visc[o], -a1a[o] * sqrt(a1));
         p_visc[o] = pmax(p_visc[o], -a2a[o] * sqrt(a2));
         p_visc[o] = pmax(p_visc[o], -a3a[o] * sqrt(a9));
-        double dx = dxb[A1(ix)], dy = dyb[A1(iy)], dz = dzb[A1(iz)];
+        double dx = dxb[A1(ix)], dy = dyb[A1(iy)] * s->hyc[A1(ix)], dz = dzb[A1(iz)] * s->hz2[H2(ix, iy)];
         visc_heat[o] =
             -0.25 * dy * dz * a1a[I3(ix, iy, iz)] * a1
             - 0.25 * dx * dz * a2a[I3(ix, iy, iz)] * a2
@@ -374,7 +421,7 @@ static void shock_viscosity(lo_state *s)
     LOOP3(0, nx, 0, ny, 0, nz)
     {
         int64_t izm = iz - 1, izp = iz + 1, iym = iy - 1, iyp = iy + 1, ixm = ix - 1, ixp = ix + 1;
-        double dx = dxb[A1(ix)], dy = dyb[A1(iy)], dz = dzb[A1(iz)];
+        double dx = dxb[A1(ix)], dy = dyb[A1(iy)] * s->hyc[A1(ix)], dz = dzb[A1(iz)] * s->hz2[H2(ix, iy)];
         double a1 = a1a[I3(ix, iyp, izp)] * dy * dz;
         double a2 = a1a[I3(ixp, iyp, izp)] * dy * dz;
         double a3 = a2a[I3(ix, iy, izp)] * dx * dz;
@@ -402,14 +449,15 @@ static void set_dt(lo_state *s)
     const double *vx = s->f[SAMS_F_VX], *vy = s->f[SAMS_F_VY], *vz = s->f[SAMS_F_VZ];
     const double *dxb = s->dxb, *dyb = s->dyb, *dzb = s->dzb;
     double best = DBL_MAX;
+    const int64_t i0 = s->p.geometry == 0 ? 0 : 1; /* lagran.cpp:384 */
 #pragma omp parallel for reduction(min : best) schedule(static)
-    for (int64_t ix = 0; ix <= nx; ++ix)
+    for (int64_t ix = i0; ix <= nx; ++ix)
         for (int64_t iy = 0; iy <= ny; ++iy)
             for (int64_t iz = 0; iz <= nz; ++iz) {
                 int64_t izm = iz - 1, iym = iy - 1, ixm = ix - 1;
                 int64_t o = I3(ix, iy, iz);
                 double dx = dxb[A1(ix)], dy = dyb[A1(iy)], dz = dzb[A1(iz)];
-                double dhx = dx, dhy = dy, dhz = dz;
+                double dhx = dx, dhy = dy * s->hyc[A1(ix)], dhz = dz * s->hzc[H2(ix, iy)];
                 double rho0 = pmax(rho[o], NONE_ZERO);
                 double cs2 = g * s->pressure[o] / rho0;
                 double w1 = (bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o]) / mu0 / rho0;
@@ -642,7 +690,10 @@ static void predictor_step(lo_state *s)
         int64_t izp = iz + 1, iyp = iy + 1, ixp = ix + 1;
         int64_t o = I3(ix, iy, iz);
         double dx = dxc[A1(ix)], dy = dyc[A1(iy)], dz = dzc[A1(iz)];
-        double dhy = dy, dhz = dz;
+        double h2 = s->hy[A1(ix)], h2x = s->hy[A1(ixp)];
+        double h3 = s->hz[H2(ix, iy)], h3x = s->hz[H2(ixp, iy)], h3y = s->hz[H2(ix, iyp)];
+        double h2c = s->hyc[A1(ix)], h3c = s->hzc[H2(ix, iy)];
+        double dhy = h2c * dy, dhz = h3c * dz;
         double pp = pressure[I3(ix, iy, iz)];
         double ppx = pressure[I3(ixp, iy, iz)];
         double ppy = pressure[I3(ix, iyp, iz)];
@@ -668,23 +719,23 @@ static void predictor_step(lo_state *s)
         double cvz = cv1[I3(ix, iy, iz)] + cv1[I3(ixp, iy, iz)] + cv1[I3(ix, iyp, iz)] + cv1[I3(ixp, iyp, iz)];
         double cvzp = cv1[I3(ix, iy, izp)] + cv1[I3(ixp, iy, izp)] + cv1[I3(ix, iyp, izp)] + cv1[I3(ixp, iyp, izp)];
 
-        w1 = (bz1[I3(ix, iy, iz)] + bz1[I3(ixp, iy, iz)] + bz1[I3(ix, iy, izp)] + bz1[I3(ixp, iy, izp)]) / cvy;
-        w2 = (bz1[I3(ix, iyp, iz)] + bz1[I3(ixp, iyp, iz)] + bz1[I3(ix, iyp, izp)] + bz1[I3(ixp, iyp, izp)]) / cvyp;
-        double jx = (w2 - w1) / dhy;
+        w1 = (bz1[I3(ix, iy, iz)] + bz1[I3(ixp, iy, iz)] + bz1[I3(ix, iy, izp)] + bz1[I3(ixp, iy, izp)]) * h3 / cvy;
+        w2 = (bz1[I3(ix, iyp, iz)] + bz1[I3(ixp, iyp, iz)] + bz1[I3(ix, iyp, izp)] + bz1[I3(ixp, iyp, izp)]) * h3y / cvyp;
+        double jx = (w2 - w1) / dhy / h3c;
         w1 = (by1[I3(ix, iy, iz)] + by1[I3(ixp, iy, iz)] + by1[I3(ix, iyp, iz)] + by1[I3(ixp, iyp, iz)]) / cvz;
         w2 = (by1[I3(ix, iy, izp)] + by1[I3(ixp, iy, izp)] + by1[I3(ix, iyp, izp)] + by1[I3(ixp, iyp, izp)]) / cvzp;
         jx -= (w2 - w1) / dhz;
 
-        w1 = (bz1[I3(ix, iy, iz)] + bz1[I3(ix, iyp, iz)] + bz1[I3(ix, iy, izp)] + bz1[I3(ix, iyp, izp)]) / cvx;
-        w2 = (bz1[I3(ixp, iy, iz)] + bz1[I3(ixp, iyp, iz)] + bz1[I3(ixp, iy, izp)] + bz1[I3(ixp, iyp, izp)]) / cvxp;
-        double jy = -(w2 - w1) / dx;
+        w1 = (bz1[I3(ix, iy, iz)] + bz1[I3(ix, iyp, iz)] + bz1[I3(ix, iy, izp)] + bz1[I3(ix, iyp, izp)]) * h3 / cvx;
+        w2 = (bz1[I3(ixp, iy, iz)] + bz1[I3(ixp, iyp, iz)] + bz1[I3(ixp, iy, izp)] + bz1[I3(ixp, iyp, izp)]) * h3x / cvxp;
+        double jy = -(w2 - w1) / dx / h3c;
         w1 = (bx1[I3(ix, iy, iz)] + bx1[I3(ixp, iy, iz)] + bx1[I3(ix, iyp, iz)] + bx1[I3(ixp, iyp, iz)]) / cvz;
         w2 = (bx1[I3(ix, iy, izp)] + bx1[I3(ixp, iy, izp)] + bx1[I3(ix, iyp, izp)] + bx1[I3(ixp, iyp, izp)]) / cvzp;
         jy += (w2 - w1) / dhz;
 
-        w1 = (by1[I3(ix, iy, iz)] + by1[I3(ix, iyp, iz)] + by1[I3(ix, iy, izp)] + by1[I3(ix, iyp, izp)]) / cvx;
-        w2 = (by1[I3(ixp, iy, iz)] + by1[I3(ixp, iyp, iz)] + by1[I3(ixp, iy, izp)] + by1[I3(ixp, iyp, izp)]) / cvxp;
-        double jz = (w2 - w1) / dx;
+        w1 = (by1[I3(ix, iy, iz)] + by1[I3(ix, iyp, iz)] + by1[I3(ix, iy, izp)] + by1[I3(ix, iyp, izp)]) * h2 / cvx;
+        w2 = (by1[I3(ixp, iy, iz)] + by1[I3(ixp, iyp, iz)] + by1[I3(ixp, iy, izp)] + by1[I3(ixp, iyp, izp)]) * h2x / cvxp;
+        double jz = (w2 - w1) / dx / h2c;
         w1 = (bx1[I3(ix, iy, iz)] + bx1[I3(ixp, iy, iz)] + bx1[I3(ix, iy, izp)] + bx1[I3(ixp, iy, izp)]) / cvy;
         w2 = (bx1[I3(ix, iyp, iz)] + bx1[I3(ixp, iyp, iz)] + bx1[I3(ix, iyp, izp)] + bx1[I3(ixp, iyp, izp)]) / cvyp;
         jz -= (w2 - w1) / dhy;
@@ -698,6 +749,17 @@ static void predictor_step(lo_state *s)
         fx += (jy * bzv - jz * byv) / mu0;
         fy += (jz * bxv - jx * bzv) / mu0;
         fz += (jx * byv - jy * bxv) / mu0;
+        /* geometry corrections (lagran.cpp:711-721) */
+        if (s->p.geometry == 2) {
+            const double cotantheta = s->cot_yb[A1(iy)], rv = s->rho_v[o], r = s->xb[A1(ix)];
+            fx += rv * (vy[o] * vy[o] + vz[o] * vz[o]) / r;
+            fy -= rv * (vy[o] * vx[o] - cotantheta * vz[o] * vz[o]) / r;
+            fz -= rv * (vz[o] * vx[o] + cotantheta * vz[o] * vy[o]) / r;
+        } else if (s->p.geometry == 1) {
+            const double rv = s->rho_v[o], r = s->xb[A1(ix)];
+            fx += rv * vy[o] * vy[o] / r;
+            fy -= rv * vy[o] * vx[o] / r;
+        }
         s->fx[o] = fx;
         s->fy[o] = fy;
         s->fz[o] = fz;
@@ -784,7 +846,7 @@ static void shock_heating(lo_state *s)
         double a11 = DD(I3(ixm, iym, izm), I3(ixm, iym, iz));
         double a12 = DD(I3(ix, iym, izm), I3(ix, iym, iz));
 #undef DD
-        double dx = dxb[A1(ix)], dy = dyb[A1(iy)], dz = dzb[A1(iz)];
+        double dx = dxb[A1(ix)], dy = dyb[A1(iy)] * s->hyc[A1(ix)], dz = dzb[A1(iz)] * s->hz2[H2(ix, iy)];
         int64_t o = I3(ix, iy, iz);
         double vh =
             (-0.25 * dy * dz * a1a[I3(ix, iy, iz)] * a1 - 0.25 * dx * dz * a2a[I3(ix, iy, iz)] * a2 - 0.25 * dy * dz * a1a[I3(ix, iyp, iz)] * a3 -
@@ -978,13 +1040,13 @@ static void sweep_volumes(lo_state *s, int dir)
             dv = (dvxdx + dvzdz) * dt;
             s->cv2[o] = vol * (1.0 + dv);
             dv = dv + dvydy * dt;
-            s->db1[o] = s->dyb[A1(iy)] + (vyb - vybm) * dt;
+            s->db1[o] = s->hyc[A1(ix)] * s->dyb[A1(iy)] + (vyb - vybm) * dt;
         } else {
             double dvxdx = xpass * tx / vol, dvydy = ypass * ty / vol, dvzdz = tz / vol;
             dv = (dvxdx + dvydy) * dt;
             s->cv2[o] = vol * (1.0 + dv);
             dv = dv + dvzdz * dt;
-            s->db1[o] = s->dzb[A1(iz)] + (vzb - vzbm) * dt;
+            s->db1[o] = s->hzc[H2(ix, iy)] * s->dzb[A1(iz)] + (vzb - vzbm) * dt;
         }
         s->cv1[o] = vol * (1.0 + dv);
     }
@@ -1312,10 +1374,11 @@ static void eulerian_remap(lo_state *s)
 
 #define ALLOC_BOX(name) do { s->name = (double *)calloc((size_t)s->nbox, sizeof(double)); if (!s->name) goto fail; } while (0)
 #define ALLOC_AX(name, n) do { s->name = (double *)calloc((size_t)((n) + 5), sizeof(double)); if (!s->name) goto fail; } while (0)
+#define ALLOC_PLANE(name) do { s->name = (double *)calloc((size_t)((p->nx + 5) * (p->ny + 5)), sizeof(double)); if (!s->name) goto fail; } while (0)
 
 lo_state *lo_create(const sams_lare_params *p, const sams_lare_bcs *bcs)
 {
-    if (!p || !bcs || p->nx < 1 || p->ny < 1 || p->nz < 1 || p->geometry != 0) return NULL;
+    if (!p || !bcs || p->nx < 1 || p->ny < 1 || p->nz < 1 || p->geometry < 0 || p->geometry > 2) return NULL;
     lo_state *s = (lo_state *)calloc(1, sizeof(lo_state));
     if (!s) return NULL;
     s->p = *p;
@@ -1331,6 +1394,8 @@ lo_state *lo_create(const sams_lare_params *p, const sams_lare_bcs *bcs)
     ALLOC_AX(xb, p->nx); ALLOC_AX(xc, p->nx); ALLOC_AX(dxb, p->nx); ALLOC_AX(dxc, p->nx);
     ALLOC_AX(yb, p->ny); ALLOC_AX(yc, p->ny); ALLOC_AX(dyb, p->ny); ALLOC_AX(dyc, p->ny);
     ALLOC_AX(zb, p->nz); ALLOC_AX(zc, p->nz); ALLOC_AX(dzb, p->nz); ALLOC_AX(dzc, p->nz);
+    ALLOC_AX(hy, p->nx); ALLOC_AX(hyc, p->nx); ALLOC_AX(hyv, p->nx); ALLOC_AX(cot_yb, p->ny);
+    ALLOC_PLANE(hz); ALLOC_PLANE(hz1); ALLOC_PLANE(hz2); ALLOC_PLANE(hzc);
     ALLOC_BOX(p_visc); ALLOC_BOX(visc_heat); ALLOC_BOX(alpha1); ALLOC_BOX(alpha2); ALLOC_BOX(alpha3);
     ALLOC_BOX(pressure); ALLOC_BOX(p_e); ALLOC_BOX(p_i); ALLOC_BOX(rho_v); ALLOC_BOX(cv_v);
     ALLOC_BOX(fx); ALLOC_BOX(fy); ALLOC_BOX(fz); ALLOC_BOX(fx_visc); ALLOC_BOX(fy_visc); ALLOC_BOX(fz_visc);
@@ -1354,6 +1419,7 @@ void lo_destroy(lo_state *s)
     for (int f = 0; f < SAMS_NFIELDS; ++f) free(s->f[f]);
     double *arrs[] = {s->cv, s->cvc, s->dxab, s->dyab, s->dzab, s->dxac, s->dyac, s->dzac,
                       s->xb, s->yb, s->zb, s->xc, s->yc, s->zc, s->dxb, s->dyb, s->dzb, s->dxc, s->dyc, s->dzc,
+                      s->hy, s->hyc, s->hyv, s->cot_yb, s->hz, s->hz1, s->hz2, s->hzc,
                       s->p_visc, s->visc_heat, s->alpha1, s->alpha2, s->alpha3, s->pressure, s->p_e, s->p_i,
                       s->rho_v, s->cv_v, s->fx, s->fy, s->fz, s->fx_visc, s->fy_visc, s->fz_visc,
                       s->bx1, s->by1, s->bz1, s->cv1, s->eta, s->flux_x, s->flux_y, s->flux_z, s->curlb,

@@ -211,7 +211,7 @@ namespace oracle
             data.t_end = 1e300;
             data.dt_snapshots = 1e300;
             data.dt_multiplier = p.dt_multiplier;
-            data.geometry = LARE::geometryType::Cartesian;
+            data.geometry = static_cast<LARE::geometryType>(p.geometry);
             data.visc1 = p.visc1;
             data.visc2 = p.visc2;
             data.gas_gamma = p.gas_gamma;
@@ -326,7 +326,9 @@ int main(int argc, char *argv[])
 {
     using namespace oracle;
     std::string dumpFinal;
-    bool quiet = false, rke = false;
+    bool quiet = false, rke = false, set_domain = false;
+    int geometry = 0;
+    double domain[6] = {0, 0, 0, 0, 0, 0};
     for (int i = 1; i < argc; ++i)
     {
         std::string a = argv[i];
@@ -351,6 +353,12 @@ int main(int argc, char *argv[])
         }
         else if (a == "--quiet") quiet = true;
         else if (a == "--rke") rke = true;
+        else if (a == "--geometry") geometry = std::atoi(arg_value(i, argc, argv));
+        else if (a == "--domain")
+        {
+            for (int d = 0; d < 6; ++d) domain[d] = std::atof(arg_value(i, argc, argv));
+            set_domain = true;
+        }
         else { std::fprintf(stderr, "unknown argument %s\n", a.c_str()); return 2; }
     }
     if (g.case_id < 0 || sams_lare_case_setup(g.case_id, g.nx, g.ny, g.nz, g.b0, &g.params, &g.bcs) != 0)
@@ -359,6 +367,13 @@ int main(int argc, char *argv[])
         return 2;
     }
     if (rke) g.params.rke = 1;  // remap kinetic-energy correction on
+    g.params.geometry = geometry;  // 0 Cartesian, 1 cylindrical, 2 spherical
+    if (set_domain)
+    {
+        g.params.x_min = domain[0]; g.params.x_max = domain[1];
+        g.params.y_min = domain[2]; g.params.y_max = domain[3];
+        g.params.z_min = domain[4]; g.params.z_max = domain[5];
+    }
     if (g.dump_step >= 0) { g.dump_file = dumpFinal; dumpFinal.clear(); }
     if (quiet) std::cout.setstate(std::ios::failbit);
 

@@ -10,6 +10,7 @@
 #include "lare_batch.cuh"
 #include "lare_ops.cuh"
 #include "lare_bc.cuh"
+#include "lare_geom_host.h"
 
 #include <algorithm>
 #include <cstring>
@@ -28,7 +29,9 @@ __device__ __forceinline__ void load_ctx(Ctx &dst, const Ctx *src)
     for (int w = threadIdx.x; w < nw; w += blockDim.x) d[w] = s[w];
 }
 
-template <class Op>
+// GEO: some solve of the batch is curvilinear (the Cartesian instantiation,
+// used when none is, carries no metric factors).
+template <class Op, bool GEO>
 __global__ void __launch_bounds__(kT, Op::kMinBlocks)
     kb_op(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int arg, int tile_i,
           int resistive_only)
@@ -49,10 +52,11 @@ __global__ void __launch_bounds__(kT, Op::kMinBlocks)
         const int j = -2 + p / ek, k = -2 + p % ek;
         if (j < lo[1] || j > hi[1] || k < lo[2] || k > hi[2]) continue;
         const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
-        for (int i = ia; i <= ib; ++i) Op::run(c, a, i, j, k);
+        for (int i = ia; i <= ib; ++i) Op::template run<GEO>(c, a, i, j, k);
     }
 }
 
+template <bool GEO>
 __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
     kb_visc(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int tile_i)
 {
@@ -74,7 +78,7 @@ __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
             if (j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
                 const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
                 for (int i = ia; i <= ib; ++i) {
-                    double cand = ops::Visc::run(c, 0, i, j, k, bad);
+                    double cand = ops::Visc::template run<GEO>(c, 0, i, j, k, bad);
                     best = dev::pmin(best, cand);
                 }
             }
@@ -305,7 +309,8 @@ int Batch::set_stream(cudaStream_t s)
 long long Batch::bytes_for(const sams_lare_params &p)
 {
     Geom g = batch_geom(p);
-    return (long long)(SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0)) * g.nelem * 8 + 8 * 2 * (p.nx + p.ny + p.nz + 18) + 256;
+    return (long long)(SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0)) * g.nelem * 8 + 8 * 2 * (p.nx + p.ny + p.nz + 18) + 256 +
+           (p.geometry ? 8LL * (long long)geom_table_size(p) : 0LL);
 }
 
 int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
@@ -314,7 +319,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
         err = "grid sizes must be in 1..60000";
         return SAMS_ERR_INVALID;
     }
-    if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.geometry < 0 || p.geometry > 2) { err = "geometry must be 0 (Cartesian), 1 (cylindrical) or 2 (spherical)"; return SAMS_ERR_UNSUPPORTED; }
     if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) { err = "empty domain"; return SAMS_ERR_INVALID; }
     {
         // tile planes and ghost shells are indexed with 32-bit integers
@@ -353,6 +358,11 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     axes_host(p.z_min, p.z_max, p.nz, dzb, dzc);
     std::vector<double> packed;
     for (auto *v : {&dxb, &dyb, &dzb, &dxc, &dyc, &dzc}) packed.insert(packed.end(), v->begin(), v->end());
+    const size_t geo_off = packed.size();
+    if (p.geometry) {  // metric factors after the spacings
+        std::vector<double> t = geom_tables(p);
+        packed.insert(packed.end(), t.begin(), t.end());
+    }
     if ((rc = check(cudaMalloc(&s.axes, packed.size() * sizeof(double)), "cudaMalloc(axes)"))) { free_slot(s); return rc; }
     if ((rc = check(cudaMemcpy(s.axes, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice), "axes"))) {
         free_slot(s);
@@ -374,6 +384,9 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
         *slots[a] = s.axes + o;
         o += lens[a];
     }
+    c.gf = GeomF{};
+    if (p.geometry) geom_bind(c.gf, s.axes + geo_off, p);
+    c.p.geometry = (int)p.geometry;
     c.p.gamma = p.gas_gamma;
     c.p.mu0 = p.mu0;
     c.p.visc1 = p.visc1;
@@ -459,6 +472,7 @@ int Batch::rebuild()
     long long shell = 0, slab[3] = {0, 0, 0};
     has_resistive_ = 0;
     has_rke_ = 0;
+    has_geo_ = 0;
     for (size_t q = 0; q < slots_.size(); ++q) {
         ctx[q] = slots_[q].ctx;
         bcs[q] = slots_[q].bc;
@@ -468,6 +482,7 @@ int Batch::rebuild()
         const Geom &g = slots_[q].ctx.g;
         has_resistive_ |= slots_[q].ctx.p.resistive;
         has_rke_ |= slots_[q].ctx.p.rke;
+        has_geo_ |= slots_[q].ctx.p.geometry != 0;
         shell_off.push_back(shell);
         const long long e0 = g.nx + 5, e1 = g.ny + 5, e2 = g.nz + 5;
         shell += 5 * e1 * e2 + (long long)g.nx * 5 * e2 + (long long)g.nx * g.ny * 5;
@@ -541,14 +556,20 @@ void Batch::launch(int arg, bool resistive_only)
 {
     if (ntiles_ == 0) return;
     const int grid = std::min(ntiles_, sm_count_ * blocks_per_sm_);
-    kb_op<Op><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, resistive_only ? 1 : 0);
+    if (has_geo_)
+        kb_op<Op, true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, resistive_only ? 1 : 0);
+    else
+        kb_op<Op, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, resistive_only ? 1 : 0);
 }
 
 void Batch::launch_visc()
 {
     if (ntiles_ == 0) return;
     const int grid = std::min(ntiles_, sm_count_ * blocks_per_sm_);
-    kb_visc<<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
+    if (has_geo_)
+        kb_visc<true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
+    else
+        kb_visc<false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
 }
 
 void Batch::bc_fill(unsigned mask, bool resistive_only)

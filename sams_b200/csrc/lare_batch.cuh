@@ -100,6 +100,7 @@ private:
     int nlive_ = 0;
     int has_resistive_ = 0;
     int has_rke_ = 0;
+    int has_geo_ = 0;
     size_t table_cap_bytes_ = 0;
     std::map<long long, cudaGraphExec_t> graphs_;
 };

@@ -55,6 +55,16 @@ struct Phys {
     double gamma, mu0, visc1, visc2_norm, dt_multiplier, eta_bg, eta0, j_max;
     int resistive;  // per-solve resistive flag (read by the batched launcher)
     int rke;        // remap kinetic-energy correction on (Ctx::dke allocated)
+    int geometry;   // 0 Cartesian, 1 cylindrical, 2 spherical (Ctx::gf set)
+};
+
+// Metric factors of a cylindrical or spherical solve, as LARE3D::grid builds
+// them (setup.cpp:277-335), computed on the host.  All null in Cartesian
+// geometry, where every factor is 1.0 and the kernels skip them.
+struct GeomF {
+    const double *hy, *hyc, *hyv, *xb;   // per x, index i + 2
+    const double *hz, *hz1, *hz2, *hzc;  // per (x, y), index (i + 2) * (ny + 5) + (j + 2)
+    const double *cot;                   // 1 / tan(yb) per y, index j + 2
 };
 
 // Per-solve device scalars.
@@ -110,6 +120,7 @@ struct Ctx {
     double *f[13];
     double *s[NSCRATCH];
     double *dke;  // delta_ke of the rke correction (null unless Phys::rke)
+    GeomF gf;     // metric factors (null in Cartesian geometry)
     Scalars *sc;
 };
 

@@ -1,0 +1,84 @@
+// lare_geom_host.h -- host tables of the cylindrical / spherical metric
+// factors (sams::GeomF), built as LARE3D::grid builds them
+// (src/PhysicsPackages/LARE/setup.cpp:277-335) from the axes of
+// axisRegistry::setDomain (include/harness/axisRegistry.h:393-430), with the
+// host's libm sin/tan like the reference, so the device sees the same bits.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "lare_device.cuh"
+#include "sams_lare_layout.h"
+
+namespace sams {
+
+// Packed layout: hy, hyc, hyv, xb (nx+5 each), hz, hz1, hz2, hzc
+// ((nx+5)(ny+5) each, index (i+2)(ny+5) + j+2), cot (ny+5).
+inline size_t geom_table_size(const sams_lare_params &p)
+{
+    const size_t X = (size_t)p.nx + 5, Y = (size_t)p.ny + 5;
+    return 4 * X + 4 * X * Y + Y;
+}
+
+inline std::vector<double> geom_tables(const sams_lare_params &p)
+{
+    const long long nx = p.nx, ny = p.ny;
+    const size_t X = (size_t)nx + 5, Y = (size_t)ny + 5, P = X * Y;
+    std::vector<double> t(geom_table_size(p), 0.0);
+    double *hy = t.data(), *hyc = hy + X, *hyv = hyc + X, *xb = hyv + X;
+    double *hz = xb + X, *hz1 = hz + P, *hz2 = hz1 + P, *hzc = hz2 + P, *cot = hzc + P;
+    auto H2 = [&](long long i, long long j) { return (size_t)((i + 2) * (long long)Y + (j + 2)); };
+    // axes: b(i) = lo + d i, c(i) = (b(i) + b(i-1)) / 2, c(-2) = 0
+    std::vector<double> xc(X), yb(Y), yc(Y);
+    const double dx = (p.x_max - p.x_min) / (double)nx, dy = (p.y_max - p.y_min) / (double)ny;
+    for (long long i = -2; i <= nx + 2; ++i) xb[i + 2] = p.x_min + dx * (double)i;
+    for (long long i = -1; i <= nx + 2; ++i) xc[i + 2] = 0.5 * (xb[i + 2] + xb[i + 1]);
+    for (long long j = -2; j <= ny + 2; ++j) yb[j + 2] = p.y_min + dy * (double)j;
+    for (long long j = -1; j <= ny + 2; ++j) yc[j + 2] = 0.5 * (yb[j + 2] + yb[j + 1]);
+    // setup.cpp:277-292; the threshold is LARE::none_zero = DBL_MIN (constants.h:43)
+    for (long long i = -2; i <= nx + 2; ++i) {
+        hy[i + 2] = std::fabs(xb[i + 2]);
+        hyc[i + 2] = std::fabs(xc[i + 2]);
+        hyv[i + 2] = (std::fabs(xc[2]) < DBL_MIN && i == 1) ? std::fabs(xc[i + 2]) : 0.25 * std::fabs(xc[i + 2]);
+    }
+    for (size_t q = 0; q < P; ++q) hz[q] = hz1[q] = hz2[q] = hzc[q] = 1.0;
+    if (p.geometry == 2) {  // setup.cpp:304-334
+        for (long long j = -2; j <= ny + 2; ++j) {
+            const double sn = std::fabs(std::sin(yb[j + 2]));
+            hz[H2(-2, j)] = hy[0] * sn;
+            for (long long i = -1; i <= nx + 2; ++i) {
+                hz[H2(i, j)] = hy[i + 2] * sn;
+                hz2[H2(i, j)] = hyc[i + 2] * sn;
+            }
+        }
+        for (long long j = -1; j <= ny + 2; ++j) {
+            const double sc = std::fabs(std::sin(yc[j + 2]));
+            hz1[H2(-2, j)] = hy[0] * sc;
+            for (long long i = -1; i <= nx + 2; ++i) {
+                hz1[H2(i, j)] = hy[i + 2] * sc;
+                hzc[H2(i, j)] = hyc[i + 2] * sc;
+            }
+        }
+        for (long long j = -2; j <= ny + 2; ++j) cot[j + 2] = 1.0 / std::tan(yb[j + 2]);  // lagran.cpp:713
+    }
+    return t;
+}
+
+// Point a GeomF at a device copy of geom_tables(p).
+inline void geom_bind(GeomF &gf, const double *dev, const sams_lare_params &p)
+{
+    const size_t X = (size_t)p.nx + 5, P = X * ((size_t)p.ny + 5);
+    gf.hy = dev;
+    gf.hyc = dev + X;
+    gf.hyv = dev + 2 * X;
+    gf.xb = dev + 3 * X;
+    gf.hz = dev + 4 * X;
+    gf.hz1 = gf.hz + P;
+    gf.hz2 = gf.hz1 + P;
+    gf.hzc = gf.hz2 + P;
+    gf.cot = gf.hzc + P;
+}
+
+}  // namespace sams

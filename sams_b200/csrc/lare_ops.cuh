@@ -42,38 +42,53 @@ using namespace dev;
 
 #define LOFF(i, j, k) box_off(g, (i), (j), (k))
 
+// Metric terms of LARE3D::grid (setup.cpp:337-390), formed on the fly: the
+// product of the 1-D spacings in the reference's order, then, outside
+// Cartesian geometry, its metric factors in the reference's order (in
+// Cartesian geometry they are 1.0 and are skipped).
+__device__ __forceinline__ int h2_index(const Ctx &c, int i, int j) { return (i + 2) * (c.g.ny + 5) + (j + 2); }
+template <bool GEO>
 __device__ __forceinline__ double cv_at(const Ctx &c, int i, int j, int k)
 {
-    return c.ax.dxb[i + 2] * (c.ax.dyb[j + 2] * c.ax.dzb[k + 2]);
+    double v = c.ax.dxb[i + 2] * (c.ax.dyb[j + 2] * c.ax.dzb[k + 2]);
+    if (GEO && c.p.geometry) v = v * c.gf.hyc[i + 2] * c.gf.hzc[h2_index(c, i, j)];
+    return v;
 }
+template <bool GEO>
 __device__ __forceinline__ double dxab_at(const Ctx &c, int i, int j, int k)
 {
-    (void)i;
-    return c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
+    double v = c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
+    if (GEO && c.p.geometry) v = v * c.gf.hy[i + 2] * c.gf.hz1[h2_index(c, i, j)];
+    return v;
 }
+template <bool GEO>
 __device__ __forceinline__ double dyab_at(const Ctx &c, int i, int j, int k)
 {
-    (void)j;
-    return c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
+    double v = c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
+    if (GEO && c.p.geometry) v = v * c.gf.hz2[h2_index(c, i, j)];
+    return v;
 }
+// dzab at k = -2 is set last with hyc (setup.cpp:368-371)
+template <bool GEO>
 __device__ __forceinline__ double dzab_at(const Ctx &c, int i, int j, int k)
 {
-    (void)k;
-    return c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
+    double v = c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
+    if (GEO && c.p.geometry) v = v * (k == -2 ? c.gf.hyc[i + 2] : c.gf.hy[i + 2]);
+    return v;
 }
+template <bool GEO>
 __device__ __forceinline__ double dxac_at(const Ctx &c, int i, int j, int k)
 {
-    (void)i;
-    return c.ax.dyb[j + 2] * c.ax.dzc[k + 2];
+    double v = c.ax.dyb[j + 2] * c.ax.dzc[k + 2];
+    if (GEO && c.p.geometry) v = v * c.gf.hyc[i + 2] * c.gf.hz2[h2_index(c, i, j)];
+    return v;
 }
+template <bool GEO>
 __device__ __forceinline__ double dyac_at(const Ctx &c, int i, int j, int k)
 {
-    (void)j;
-    return c.ax.dxb[i + 2] * c.ax.dzc[k + 2];
-}
-__device__ __forceinline__ double cvc_at(const Ctx &c, int i, int j, int k)
-{
-    return c.ax.dxb[i + 2] * (c.ax.dyb[j + 2] * c.ax.dzc[k + 2]);
+    double v = c.ax.dxb[i + 2] * c.ax.dzc[k + 2];
+    if (GEO && c.p.geometry) v = v * c.gf.hz1[h2_index(c, i, j)];
+    return v;
 }
 
 __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int a1, int b1, int a2, int b2)
@@ -98,6 +113,7 @@ struct CellPrep {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -128,13 +144,14 @@ struct NodePrep {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
         const RO rho{c.f[SAMS_F_RHO]}, cs{c.s[S_CS]};
         const int ip = i + 1, jp = j + 1, kp = k + 1;
-        double cv0 = cv_at(c, i, j, k), cv1 = cv_at(c, ip, j, k), cv2 = cv_at(c, i, jp, k), cv3 = cv_at(c, ip, jp, k);
-        double cv4 = cv_at(c, i, j, kp), cv5 = cv_at(c, ip, j, kp), cv6 = cv_at(c, i, jp, kp), cv7 = cv_at(c, ip, jp, kp);
+        double cv0 = cv_at<GEO>(c, i, j, k), cv1 = cv_at<GEO>(c, ip, j, k), cv2 = cv_at<GEO>(c, i, jp, k), cv3 = cv_at<GEO>(c, ip, jp, k);
+        double cv4 = cv_at<GEO>(c, i, j, kp), cv5 = cv_at<GEO>(c, ip, j, kp), cv6 = cv_at<GEO>(c, i, jp, kp), cv7 = cv_at<GEO>(c, ip, jp, kp);
         int o0 = LOFF(i, j, k), o1 = LOFF(ip, j, k), o2 = LOFF(i, jp, k), o3 = LOFF(ip, jp, k);
         int o4 = LOFF(i, j, kp), o5 = LOFF(ip, j, kp), o6 = LOFF(i, jp, kp), o7 = LOFF(ip, jp, kp);
         double sum_rho_cv = rho[o0] * cv0 + rho[o1] * cv1 + rho[o2] * cv2 + rho[o3] * cv3 +
@@ -156,6 +173,7 @@ struct Alpha {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -175,6 +193,10 @@ struct Alpha {
             int o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
             int o0 = o1 - g.sy, o3 = o2 + g.sy;
             double dx = c.ax.dyb[j + 2], dxp = c.ax.dyb[j + 3], dxm = c.ax.dyb[j + 1];
+            if (GEO && c.p.geometry) {  // lagran.cpp:251-253
+                const double h = c.gf.hy[i + 2];
+                dx = dx * h; dxp = dxp * h; dxm = dxm * h;
+            }
             double dvdots = -(vy[o1] - vy[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A2][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
@@ -183,6 +205,10 @@ struct Alpha {
             int o1 = o - 1, o2 = o;
             int o0 = o1 - 1, o3 = o2 + 1;
             double dx = c.ax.dzb[k + 2], dxp = c.ax.dzb[k + 3], dxm = c.ax.dzb[k + 1];
+            if (GEO && c.p.geometry) {  // lagran.cpp:270-272
+                const double h = c.gf.hz[h2_index(c, i, j)];
+                dx = dx * h; dxp = dxp * h; dxm = dxm * h;
+            }
             double dvdots = -(vz[o1] - vz[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A3][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
@@ -202,6 +228,7 @@ struct Visc {
     // nonfinite is set when a NaN or infinity shows up in this cell's viscous
     // pressure, heating or CFL terms (the solve's state is no longer finite;
     // the min itself would hide it, as LARE's min does).
+    template <bool GEO>
     __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
     {
         const Geom &g = c.g;
@@ -209,7 +236,10 @@ struct Visc {
         const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
         const int SX = g.sx, SY = g.sy;
         const int o = LOFF(i, j, k);
-        const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
+        const double dx = c.ax.dxb[i + 2], dyp = c.ax.dyb[j + 2], dzp = c.ax.dzb[k + 2];
+        // edge lengths of the heating and forces (lagran.cpp:307-309, 338-340)
+        const double dy = (GEO && c.p.geometry) ? dyp * c.gf.hyc[i + 2] : dyp;
+        const double dz = (GEO && c.p.geometry) ? dzp * c.gf.hz2[h2_index(c, i, j)] : dzp;
 #define DV2(a, b) ((vx[a] - vx[b]) * (vx[a] - vx[b]) + (vy[a] - vy[b]) * (vy[a] - vy[b]) + (vz[a] - vz[b]) * (vz[a] - vz[b]))
         // cell (ix, iy, iz) corners: m = minus one along that axis
         const int c_mmm = o - SX - SY - 1, c_0mm = o - SY - 1, c_00m = o - 1, c_m0m = o - SX - 1;
@@ -243,7 +273,7 @@ struct Visc {
                     - 0.25 * dx * dy * a3a[o - SX] * a10
                     - 0.25 * dx * dy * a3a[o - SX - SY] * a11
                     - 0.25 * dx * dy * a3a[o - SY] * a12;
-        const double cv = dx * (dy * dz);
+        const double cv = (GEO && c.p.geometry) ? cv_at<GEO>(c, i, j, k) : dx * (dyp * dzp);
         c.s[S_VH][o] = vh / cv;
         if (i > g.nx || j > g.ny || k > g.nz) return DBL_MAX;
 
@@ -257,8 +287,8 @@ struct Visc {
             double e6 = a3a[o + 1] * dx * dy;
             // cv_v = 0.125 * (8-cell sum of cv) (lagran.cpp:142-151)
             const int ip = i + 1, jp = j + 1, kp = k + 1;
-            double sum_cv = cv_at(c, i, j, k) + cv_at(c, ip, j, k) + cv_at(c, i, jp, k) + cv_at(c, ip, jp, k) +
-                            cv_at(c, i, j, kp) + cv_at(c, ip, j, kp) + cv_at(c, i, jp, kp) + cv_at(c, ip, jp, kp);
+            double sum_cv = cv_at<GEO>(c, i, j, k) + cv_at<GEO>(c, ip, j, k) + cv_at<GEO>(c, i, jp, k) + cv_at<GEO>(c, ip, jp, k) +
+                            cv_at<GEO>(c, i, j, kp) + cv_at<GEO>(c, ip, j, kp) + cv_at<GEO>(c, i, jp, kp) + cv_at<GEO>(c, ip, jp, kp);
             double cv_v = 0.125 * sum_cv;
 #define FV(v) ((e1 * (v[o] - v[o - SX]) + e2 * (v[o] - v[o + SX]) + e3 * (v[o] - v[o - SY]) + \
                 e4 * (v[o] - v[o + SY]) + e5 * (v[o] - v[o - 1]) + e6 * (v[o] - v[o + 1])) / cv_v)
@@ -277,9 +307,19 @@ struct Visc {
         double cs2 = gm * pressure / rho0;
         double w1 = (bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o]) / c.p.mu0 / rho0;
         double c_visc2 = p_visc / rho0;
-        double length = pmin(pmin(dx, dy), dz);
+        // outside Cartesian geometry the CFL range starts at x index 1 (lagran.cpp:384)
+        if (GEO && c.p.geometry && i < 1) return DBL_MAX;
+        // lagran.cpp:396-398
+        const double dhy = (GEO && c.p.geometry) ? dyp * c.gf.hyc[i + 2] : dyp;
+        const double dhz = (GEO && c.p.geometry) ? dzp * c.gf.hzc[h2_index(c, i, j)] : dzp;
+        double length = pmin(pmin(dx, dhy), dhz);
         double dt1 = length / (sqrt(c_visc2) + sqrt(cs2 + w1 + c_visc2));
-        double ax = 0.25 * (dy * dz), ay = 0.25 * (dx * dz), az = 0.25 * (dx * dy);
+        double ax = 0.25 * (dyp * dzp), ay = 0.25 * (dx * dzp), az = 0.25 * (dx * dyp);
+        if (GEO && c.p.geometry) {  // lagran.cpp:404-406 reads the metric arrays
+            ax = 0.25 * dxab_at<GEO>(c, i, j, k);
+            ay = 0.25 * dyab_at<GEO>(c, i, j, k);
+            az = 0.25 * dzab_at<GEO>(c, i, j, k);
+        }
         double vxbm = (vx[c_m00] + vx[c_mm0] + vx[c_m0m] + vx[c_mmm]) * ax;
         double vxbp = (vx[c_000] + vx[c_0m0] + vx[c_00m] + vx[c_0mm]) * ax;
         double vybm = (vy[c_0m0] + vy[c_mm0] + vy[c_0mm] + vy[c_mmm]) * ay;
@@ -308,6 +348,7 @@ struct ResistRK {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -339,6 +380,7 @@ struct ResistB {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int last, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -384,19 +426,16 @@ struct Pred1 {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const double dt = c.sc->dt;
-        const double dxb0 = c.ax.dxb[i + 2], dxbm = c.ax.dxb[i + 1];
-        const double dyb0 = c.ax.dyb[j + 2], dybm = c.ax.dyb[j + 1];
-        const double dzb0 = c.ax.dzb[k + 2], dzbm = c.ax.dzb[k + 1];
-        const double dxab0 = dyb0 * dzb0, dxabm = dyb0 * dzb0;          // dxab(i) and dxab(i-1)
-        const double dyab0 = dxb0 * dzb0, dyabm = dxb0 * dzb0;          // dyab(j) and dyab(j-1)
-        const double dzab0 = dxb0 * dyb0, dzabm = dxb0 * dyb0;          // dzab(k) and dzab(k-1)
-        (void)dxbm; (void)dybm; (void)dzbm;
+        const double dxab0 = dxab_at<GEO>(c, i, j, k), dxabm = dxab_at<GEO>(c, i - 1, j, k);
+        const double dyab0 = dyab_at<GEO>(c, i, j, k), dyabm = dyab_at<GEO>(c, i, j - 1, k);
+        const double dzab0 = dzab_at<GEO>(c, i, j, k), dzabm = dzab_at<GEO>(c, i, j, k - 1);
         const int a = o, am = o - SX, bm = o - SY, cm = o - 1;
         double vxb = 0.25 * (vx[a] + vx[bm] + vx[cm] + vx[bm - 1]);
         double vxbm = 0.25 * (vx[am] + vx[am - SY] + vx[am - 1] + vx[am - SY - 1]);
@@ -404,7 +443,7 @@ struct Pred1 {
         double vybm = 0.25 * (vy[bm] + vy[bm - SX] + vy[bm - 1] + vy[bm - SX - 1]);
         double vzb = 0.25 * (vz[a] + vz[am] + vz[bm] + vz[am - SY]);
         double vzbm = 0.25 * (vz[cm] + vz[am - 1] + vz[bm - 1] + vz[am - SY - 1]);
-        double vol = dxb0 * (dyb0 * dzb0);
+        double vol = cv_at<GEO>(c, i, j, k);
         double dvxdx = (vxb * dxab0 - vxbm * dxabm) / vol;
         double dvydy = (vyb * dyab0 - vybm * dyabm) / vol;
         double dvzdz = (vzb * dzab0 - vzbm * dzabm) / vol;
@@ -477,6 +516,7 @@ struct Pred2 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -484,7 +524,19 @@ struct Pred2 {
         const RO pe{c.s[S_PE]}, pi{c.s[S_PI]}, cv1{c.s[S_CV1]};
         const RO bx1{c.s[S_B1X]}, by1{c.s[S_B1Y]}, bz1{c.s[S_B1Z]};
         const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
-        const double dhy = dy, dhz = dz;
+        // metric factors (lagran.cpp:627-630; all 1.0 in Cartesian geometry)
+        const bool geo = GEO && c.p.geometry != 0;
+        double h2 = 1.0, h2x = 1.0, h3 = 1.0, h3x = 1.0, h3y = 1.0, h2c = 1.0, h3c = 1.0;
+        if (geo) {
+            h2 = c.gf.hy[i + 2];
+            h2x = c.gf.hy[i + 3];
+            h3 = c.gf.hz[h2_index(c, i, j)];
+            h3x = c.gf.hz[h2_index(c, i + 1, j)];
+            h3y = c.gf.hz[h2_index(c, i, j + 1)];
+            h2c = c.gf.hyc[i + 2];
+            h3c = c.gf.hzc[h2_index(c, i, j)];
+        }
+        const double dhy = geo ? h2c * dy : dy, dhz = geo ? h3c * dz : dz;
         const int q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
                         qyz = o + SY + 1, qxyz = o + SX + SY + 1;
         double pp = pe[q0] + pi[q0], ppx = pe[qx] + pi[qx], ppy = pe[qy] + pi[qy], ppz = pe[qz] + pi[qz];
@@ -506,23 +558,44 @@ struct Pred2 {
         double cvz = cv1[q0] + cv1[qx] + cv1[qy] + cv1[qxy];
         double cvzp = cv1[qz] + cv1[qxz] + cv1[qyz] + cv1[qxyz];
 
-        w1 = (bz1[q0] + bz1[qx] + bz1[qz] + bz1[qxz]) / cvy;
-        w2 = (bz1[qy] + bz1[qxy] + bz1[qyz] + bz1[qxyz]) / cvyp;
-        double jx = (w2 - w1) / dhy;
+        double jx;
+        if (geo) {
+            w1 = (bz1[q0] + bz1[qx] + bz1[qz] + bz1[qxz]) * h3 / cvy;
+            w2 = (bz1[qy] + bz1[qxy] + bz1[qyz] + bz1[qxyz]) * h3y / cvyp;
+            jx = (w2 - w1) / dhy / h3c;
+        } else {
+            w1 = (bz1[q0] + bz1[qx] + bz1[qz] + bz1[qxz]) / cvy;
+            w2 = (bz1[qy] + bz1[qxy] + bz1[qyz] + bz1[qxyz]) / cvyp;
+            jx = (w2 - w1) / dhy;
+        }
         w1 = (by1[q0] + by1[qx] + by1[qy] + by1[qxy]) / cvz;
         w2 = (by1[qz] + by1[qxz] + by1[qyz] + by1[qxyz]) / cvzp;
         jx -= (w2 - w1) / dhz;
 
-        w1 = (bz1[q0] + bz1[qy] + bz1[qz] + bz1[qyz]) / cvx;
-        w2 = (bz1[qx] + bz1[qxy] + bz1[qxz] + bz1[qxyz]) / cvxp;
-        double jy = -(w2 - w1) / dx;
+        double jy;
+        if (geo) {
+            w1 = (bz1[q0] + bz1[qy] + bz1[qz] + bz1[qyz]) * h3 / cvx;
+            w2 = (bz1[qx] + bz1[qxy] + bz1[qxz] + bz1[qxyz]) * h3x / cvxp;
+            jy = -(w2 - w1) / dx / h3c;
+        } else {
+            w1 = (bz1[q0] + bz1[qy] + bz1[qz] + bz1[qyz]) / cvx;
+            w2 = (bz1[qx] + bz1[qxy] + bz1[qxz] + bz1[qxyz]) / cvxp;
+            jy = -(w2 - w1) / dx;
+        }
         w1 = (bx1[q0] + bx1[qx] + bx1[qy] + bx1[qxy]) / cvz;
         w2 = (bx1[qz] + bx1[qxz] + bx1[qyz] + bx1[qxyz]) / cvzp;
         jy += (w2 - w1) / dhz;
 
-        w1 = (by1[q0] + by1[qy] + by1[qz] + by1[qyz]) / cvx;
-        w2 = (by1[qx] + by1[qxy] + by1[qxz] + by1[qxyz]) / cvxp;
-        double jz = (w2 - w1) / dx;
+        double jz;
+        if (geo) {
+            w1 = (by1[q0] + by1[qy] + by1[qz] + by1[qyz]) * h2 / cvx;
+            w2 = (by1[qx] + by1[qxy] + by1[qxz] + by1[qxyz]) * h2x / cvxp;
+            jz = (w2 - w1) / dx / h2c;
+        } else {
+            w1 = (by1[q0] + by1[qy] + by1[qz] + by1[qyz]) / cvx;
+            w2 = (by1[qx] + by1[qxy] + by1[qxz] + by1[qxyz]) / cvxp;
+            jz = (w2 - w1) / dx;
+        }
         w1 = (bx1[q0] + bx1[qx] + bx1[qz] + bx1[qxz]) / cvy;
         w2 = (bx1[qy] + bx1[qxy] + bx1[qyz] + bx1[qxyz]) / cvyp;
         jz -= (w2 - w1) / dhy;
@@ -536,6 +609,19 @@ struct Pred2 {
         fx += (jy * bzv - jz * byv) / mu0;
         fy += (jz * bxv - jx * bzv) / mu0;
         fz += (jx * byv - jy * bxv) / mu0;
+        if (geo) {  // geometric source terms (lagran.cpp:711-721)
+            const double rv = __ldg(c.s[S_RHOV] + o), r = c.gf.xb[i + 2];
+            const double ux = __ldg(c.f[SAMS_F_VX] + o), uy = __ldg(c.f[SAMS_F_VY] + o), uz = __ldg(c.f[SAMS_F_VZ] + o);
+            if (c.p.geometry == 2) {
+                const double cotantheta = c.gf.cot[j + 2];
+                fx += rv * (uy * uy + uz * uz) / r;
+                fy -= rv * (uy * ux - cotantheta * uz * uz) / r;
+                fz -= rv * (uz * ux + cotantheta * uz * uy) / r;
+            } else {
+                fx += rv * uy * uy / r;
+                fy -= rv * uy * ux / r;
+            }
+        }
         c.s[S_FX][o] = fx;
         c.s[S_FY][o] = fy;
         c.s[S_FZ][o] = fz;
@@ -555,6 +641,7 @@ struct Corr1 {
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -578,12 +665,17 @@ struct Corr1 {
         double a11 = DD(mm0 - 1, mm0);
         double a12 = DD(om0 - 1, om0);
 #undef DD
-        const double dx = c.ax.dxb[i + 2], dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
+        const double dx = c.ax.dxb[i + 2];
+        double dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
+        if (GEO && c.p.geometry) {  // lagran.cpp:980-982
+            dy = dy * c.gf.hyc[i + 2];
+            dz = dz * c.gf.hz2[h2_index(c, i, j)];
+        }
         double vh = (-0.25 * dy * dz * a1a[o] * a1 - 0.25 * dx * dz * a2a[o] * a2 - 0.25 * dy * dz * a1a[o + SY] * a3 -
                      0.25 * dx * dz * a2a[o - SX] * a4 - 0.25 * dy * dz * a1a[o + 1] * a5 - 0.25 * dx * dz * a2a[o + 1] * a6 -
                      0.25 * dy * dz * a1a[o + SY + 1] * a7 - 0.25 * dx * dz * a2a[o - SX + 1] * a8 - 0.25 * dy * dy * a3a[o] * a9 -
                      0.25 * dx * dy * a3a[o - SX] * a10 - 0.25 * dy * dy * a3a[o - SX - SY] * a11 - 0.25 * dx * dy * a3a[o - SY] * a12);
-        c.s[S_VH][o] = pmax(vh / (dx * (dy * dz)), 0.0);
+        c.s[S_VH][o] = pmax(vh / cv_at<GEO>(c, i, j, k), 0.0);
     }
 };
 
@@ -596,6 +688,7 @@ struct Corr2 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -617,11 +710,10 @@ struct Corr2 {
         double vybm = 0.25 * (vy1[bm] + vy1[bm - SX] + vy1[bm - 1] + vy1[bm - SX - 1]);
         double vzb = 0.25 * (vz1[a] + vz1[am] + vz1[bm] + vz1[am - SY]);
         double vzbm = 0.25 * (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]);
-        const double dxb0 = c.ax.dxb[i + 2], dyb0 = c.ax.dyb[j + 2], dzb0 = c.ax.dzb[k + 2];
-        double vol = dxb0 * (dyb0 * dzb0);
-        double dvxdx = (vxb * (dyb0 * dzb0) - vxbm * (dyb0 * dzb0)) / vol;
-        double dvydy = (vyb * (dxb0 * dzb0) - vybm * (dxb0 * dzb0)) / vol;
-        double dvzdz = (vzb * (dxb0 * dyb0) - vzbm * (dxb0 * dyb0)) / vol;
+        double vol = cv_at<GEO>(c, i, j, k);
+        double dvxdx = (vxb * dxab_at<GEO>(c, i, j, k) - vxbm * dxab_at<GEO>(c, i - 1, j, k)) / vol;
+        double dvydy = (vyb * dyab_at<GEO>(c, i, j, k) - vybm * dyab_at<GEO>(c, i, j - 1, k)) / vol;
+        double dvzdz = (vzb * dzab_at<GEO>(c, i, j, k) - vzbm * dzab_at<GEO>(c, i, j, k - 1)) / vol;
         double dv = (dvxdx + dvydy + dvzdz) * dt;
         double *rho = c.f[SAMS_F_RHO], *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
         double r = rho[o];
@@ -643,22 +735,23 @@ struct BScale {
     {
         set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int back, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
         if (j >= -1 && k >= -1) {
-            double a = dxab_at(c, i, j, k);
+            double a = dxab_at<GEO>(c, i, j, k);
             double *b = c.f[SAMS_F_BX];
             b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
         }
         if (i >= -1 && k >= -1) {
-            double a = dyab_at(c, i, j, k);
+            double a = dyab_at<GEO>(c, i, j, k);
             double *b = c.f[SAMS_F_BY];
             b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
         }
         if (i >= -1 && j >= -1) {
-            double a = dzab_at(c, i, j, k);
+            double a = dzab_at<GEO>(c, i, j, k);
             double *b = c.f[SAMS_F_BZ];
             b[o] = back ? b[o] / (a + NONE_ZERO) : b[o] * a;
         }
@@ -682,32 +775,33 @@ struct SweepVol {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
         const double dxb0 = c.ax.dxb[i + 2], dyb0 = c.ax.dyb[j + 2], dzb0 = c.ax.dzb[k + 2];
-        const double vol = dxb0 * (dyb0 * dzb0);
+        const double vol = cv_at<GEO>(c, i, j, k);
         const int am = o - SX, bm = o - SY, cm = o - 1;
         double tx = 0.0, ty = 0.0, tz = 0.0, vxb = 0.0, vxbm = 0.0, vyb = 0.0, vybm = 0.0, vzb = 0.0, vzbm = 0.0;
         if (DIR == 0) {
             const RO vx1{c.f[SAMS_F_VX1]};
             vxb = (vx1[o] + vx1[bm] + vx1[cm] + vx1[bm - 1]) * 0.25;
             vxbm = (vx1[am] + vx1[am - SY] + vx1[am - 1] + vx1[am - SY - 1]) * 0.25;
-            tx = vxb * (dyb0 * dzb0) - vxbm * (dyb0 * dzb0);
+            tx = vxb * dxab_at<GEO>(c, i, j, k) - vxbm * dxab_at<GEO>(c, i - 1, j, k);
         }
         if (DIR <= 1) {
             const RO vy1{c.f[SAMS_F_VY1]};
             vyb = (vy1[o] + vy1[am] + vy1[cm] + vy1[am - 1]) * 0.25;
             vybm = (vy1[bm] + vy1[bm - SX] + vy1[bm - 1] + vy1[bm - SX - 1]) * 0.25;
-            ty = vyb * (dxb0 * dzb0) - vybm * (dxb0 * dzb0);
+            ty = vyb * dyab_at<GEO>(c, i, j, k) - vybm * dyab_at<GEO>(c, i, j - 1, k);
         }
         {
             const RO vz1{c.f[SAMS_F_VZ1]};
             vzb = (vz1[o] + vz1[am] + vz1[bm] + vz1[am - SY]) * 0.25;
             vzbm = (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]) * 0.25;
-            tz = vzb * (dxb0 * dyb0) - vzbm * (dxb0 * dyb0);
+            tz = vzb * dzab_at<GEO>(c, i, j, k) - vzbm * dzab_at<GEO>(c, i, j, k - 1);
         }
         double dv, cv2, db1;
         if (DIR == 0) {
@@ -721,13 +815,15 @@ struct SweepVol {
             dv = dvzdz * dt;
             cv2 = vol * (1.0 + dv);
             dv = dv + dvydy * dt;
-            db1 = dyb0 + (vyb - vybm) * dt;
+            // hyc * dyb (yremap.cpp:78); hyc = 1 in Cartesian geometry
+            db1 = ((GEO && c.p.geometry) ? c.gf.hyc[i + 2] * dyb0 : dyb0) + (vyb - vybm) * dt;
         } else {
             double dvzdz = tz / vol;
             dv = 0.0 * dt;
             cv2 = vol * (1.0 + dv);
             dv = dv + dvzdz * dt;
-            db1 = dzb0 + (vzb - vzbm) * dt;
+            // hzc * dzb (zremap.cpp:79)
+            db1 = ((GEO && c.p.geometry) ? c.gf.hzc[h2_index(c, i, j)] * dzb0 : dzb0) + (vzb - vzbm) * dt;
         }
         c.s[S_R_CV2][o] = cv2;
         c.s[S_R_CV1][o] = vol * (1.0 + dv);
@@ -743,6 +839,7 @@ struct SweepCvc {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -761,6 +858,7 @@ struct SweepCT {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -810,6 +908,7 @@ struct SweepCTUpd {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -861,10 +960,10 @@ __device__ __forceinline__ double face_velocity(const Ctx &c, int o)
     }
 }
 
-template <int DIR>
+template <int DIR, bool GEO>
 __device__ __forceinline__ double face_area(const Ctx &c, int i, int j, int k)
 {
-    return DIR == 0 ? dxab_at(c, i, j, k) : (DIR == 1 ? dyab_at(c, i, j, k) : dzab_at(c, i, j, k));
+    return DIR == 0 ? dxab_at<GEO>(c, i, j, k) : (DIR == 1 ? dyab_at<GEO>(c, i, j, k) : dzab_at<GEO>(c, i, j, k));
 }
 
 template <int DIR>
@@ -875,6 +974,7 @@ struct SweepMass {
         set_bounds(lo, hi, 0, DIR == 0 ? g.nx : g.nx + 1, 0, DIR == 1 ? g.ny : g.ny + 1, 0,
                    DIR == 2 ? g.nz : g.nz + 1);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -882,7 +982,7 @@ struct SweepMass {
         const int d = dir_stride(g, DIR);
         const RO rho{c.f[SAMS_F_RHO]}, cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
         double v = face_velocity<DIR>(c, o);
-        c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
+        c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
                                       rho[o + 2 * d], cvc1[o], cvc1[o - d], cvc1[o + d], cv1[o], cv1[o + d]);
     }
 };
@@ -905,6 +1005,7 @@ struct SweepS6 {
         set_bounds(lo, hi, DIR == 0 ? -2 : 0, DIR == 0 ? g.nx + 1 : g.nx, DIR == 1 ? -2 : 0,
                    DIR == 1 ? g.ny + 1 : g.ny, DIR == 2 ? -2 : 0, DIR == 2 ? g.nz + 1 : g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -922,7 +1023,7 @@ struct SweepS6 {
         // energy fluxes (0..n)^3
         if (all0n) {
             double v = face_velocity<DIR>(c, o);
-            double area = face_area<DIR>(c, i, j, k);
+            double area = face_area<DIR, GEO>(c, i, j, k);
             const RO ee{c.f[SAMS_F_ENERGY_ELECTRON]}, ei{c.f[SAMS_F_ENERGY_ION]};
             c.s[S_R_FE1][o] = energy_flux(v, dt, area, ee[o - d], ee[o], ee[o + d], ee[o + 2 * d], cvc1[o], cvc1[o - d],
                                           cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]);
@@ -961,6 +1062,7 @@ struct SweepS7 {
     {
         set_bounds(lo, hi, DIR == 0 ? -1 : 0, g.nx, DIR == 1 ? -1 : 0, g.ny, DIR == 2 ? -1 : 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -977,7 +1079,7 @@ struct SweepS7 {
         }
         const RO v1s{c.s[S_R_V1S]}, rv{c.s[S_R_RVN]}, dmn{c.s[S_R_DMN]};
         // x sweep uses dxac; the y and z sweeps both use dyac (zremap.cpp:475)
-        double area = DIR == 0 ? dxac_at(c, i, j, k) : dyac_at(c, i, j, k);
+        double area = DIR == 0 ? dxac_at<GEO>(c, i, j, k) : dyac_at<GEO>(c, i, j, k);
         const double v = v1s[o], dmv = dmn[o];
         const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
         const double rvi = rv[o], rvp = rv[o + d];
@@ -1006,6 +1108,7 @@ struct SweepS8 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -1041,6 +1144,7 @@ struct RkeZero {
     {
         set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (c.p.rke) c.dke[box_off(c.g, i, j, k)] = 0.0;
@@ -1060,6 +1164,7 @@ struct SweepRkeDk {
         set_bounds(lo, hi, 0, DIR == 0 ? g.nx - 1 : g.nx, 0, DIR == 1 ? g.ny - 1 : g.ny, 0,
                    DIR == 2 ? g.nz - 1 : g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;
@@ -1099,6 +1204,7 @@ struct SweepRkeGather {
         set_bounds(lo, hi, DIR == 0 ? 1 : 0, DIR == 0 ? g.nx : g.nx + 1, DIR == 1 ? 1 : 0,
                    DIR == 1 ? g.ny : g.ny + 1, DIR == 2 ? 1 : 0, DIR == 2 ? g.nz : g.nz + 1);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;
@@ -1138,12 +1244,13 @@ struct RkeEnergy {
     {
         set_bounds(lo, hi, 1, g.nx, 1, g.ny, 1, g.nz);
     }
+    template <bool GEO>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
-        const double d = pmax(-c.dke[o], 0.0) / (__ldg(c.f[SAMS_F_RHO] + o) * cv_at(c, i, j, k));
+        const double d = pmax(-c.dke[o], 0.0) / (__ldg(c.f[SAMS_F_RHO] + o) * cv_at<GEO>(c, i, j, k));
         double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
         ee[o] += 0.5 * d;
         ei[o] += 0.5 * d;

@@ -261,8 +261,8 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
         sams_capi_set_last_error("sams_lare_serve_submit: invalid argument");
         return SAMS_ERR_INVALID;
     }
-    if (p->geometry != 0) {
-        sams_capi_set_last_error("sams_lare_serve_submit: only Cartesian geometry is built");
+    if (p->geometry < 0 || p->geometry > 2) {
+        sams_capi_set_last_error("sams_lare_serve_submit: geometry must be 0, 1 or 2");
         return SAMS_ERR_UNSUPPORTED;
     }
     auto r = std::make_unique<Request>();

@@ -16,6 +16,7 @@
 #include "lare_solver.cuh"
 #include "lare_ops.cuh"
 #include "lare_bc.cuh"
+#include "lare_geom_host.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -27,8 +28,10 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// One thread per (j, k) of a plane, blockIdx.y walks i.
-template <class Op>
+// One thread per (j, k) of a plane, blockIdx.y walks i.  GEO: the solve's
+// geometry is curvilinear (its metric factors are applied); the Cartesian
+// instantiation has no trace of them.
+template <class Op, bool GEO>
 __global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
 {
     int lo[3], hi[3];
@@ -39,12 +42,13 @@ __global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
     if (t >= plane) return;
     const int j = lo[1] + (int)(t / nk);
     const int k = lo[2] + (int)(t % nk);
-    for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::run(c, arg, i, j, k);
+    for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::template run<GEO>(c, arg, i, j, k);
 }
 
 // Visc with the CFL minimum: each block reduces its candidates and folds
 // them into Scalars::dtmin_bits.  Positive doubles order like their bit
 // patterns, so an integer atomicMin is an exact, order-free minimum.
+template <bool GEO>
 __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
 {
     int lo[3], hi[3];
@@ -58,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
         const int j = lo[1] + (int)(t / nk);
         const int k = lo[2] + (int)(t % nk);
         for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) {
-            double cand = ops::Visc::run(c, 0, i, j, k, bad);
+            double cand = ops::Visc::template run<GEO>(c, 0, i, j, k, bad);
             best = dev::pmin(best, cand);
         }
     }
@@ -254,7 +258,7 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
 {
     if (p.nx < 1 || p.ny < 1 || p.nz < 1) { err = "grid sizes must be >= 1"; return SAMS_ERR_INVALID; }
     if (p.nx > 60000 || p.ny > 60000 || p.nz > 60000) { err = "grid size too large"; return SAMS_ERR_INVALID; }
-    if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.geometry < 0 || p.geometry > 2) { err = "geometry must be 0 (Cartesian), 1 (cylindrical) or 2 (spherical)"; return SAMS_ERR_UNSUPPORTED; }
     if (!(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min)) {
         err = "empty domain";
         return SAMS_ERR_INVALID;
@@ -306,6 +310,11 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     axis_host(p.z_min, p.z_max, p.nz, dzb, dzc);
     std::vector<double> packed;
     for (auto *v : {&dxb, &dyb, &dzb, &dxc, &dyc, &dzc}) packed.insert(packed.end(), v->begin(), v->end());
+    const size_t geo_off = packed.size();
+    if (p.geometry) {  // metric factors after the spacings
+        std::vector<double> t = geom_tables(p);
+        packed.insert(packed.end(), t.begin(), t.end());
+    }
     if ((rc = check(cudaMalloc(&axes_, packed.size() * sizeof(double)), "cudaMalloc(axes)"))) return rc;
     if ((rc = check(cudaMemcpy(axes_, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice), "axes upload"))) return rc;
     size_t off = 0;
@@ -315,6 +324,9 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
         *slots[a] = axes_ + off;
         off += lens[a];
     }
+    ctx_.gf = GeomF{};
+    if (p.geometry) geom_bind(ctx_.gf, axes_ + geo_off, p);
+    ctx_.p.geometry = (int)p.geometry;
 
     ctx_.p.gamma = p.gas_gamma;
     ctx_.p.mu0 = p.mu0;
@@ -340,7 +352,10 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
 int Solver::init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, const Ctx &ctx, int device,
                           cudaStream_t stream)
 {
-    if (p.geometry != 0) { err = "only Cartesian geometry is built"; return SAMS_ERR_UNSUPPORTED; }
+    if (p.geometry != 0) {
+        err = "only Cartesian geometry is available on this entry point (no room for the metric tables)";
+        return SAMS_ERR_UNSUPPORTED;
+    }
     if (p.rke != 0) {
         err = "the remap kinetic-energy correction (rke) needs an array this entry point does not have";
         return SAMS_ERR_UNSUPPORTED;
@@ -454,7 +469,10 @@ void Solver::launch(int arg)
     Op::bounds(ctx_.g, arg, lo, hi);
     const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
     dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(hi[0] - lo[0] + 1));
-    k_op<Op><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+    if (p_.geometry)
+        k_op<Op, true><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+    else
+        k_op<Op, false><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
     ++launches_;
 }
 
@@ -520,7 +538,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
         const int ni = hi[0] - lo[0] + 1;
         dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(ni < 16 ? ni : 16));
-        k_visc<<<grid, kThreads, 0, stream_>>>(ctx_);
+        if (p_.geometry)
+            k_visc<true><<<grid, kThreads, 0, stream_>>>(ctx_);
+        else
+            k_visc<false><<<grid, kThreads, 0, stream_>>>(ctx_);
         ++launches_;
     }
     k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);

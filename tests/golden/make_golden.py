@@ -23,7 +23,9 @@ from oracle import lare_oracle as lo  # noqa: E402
 from oracle import dumpio  # noqa: E402
 from oracle.dumpio import Dump  # noqa: E402
 
-# (name, case, nx, ny, nz, steps, seed, b0[, rke])
+GEO_DOMAIN = [1.0, 2.0, 0.5, 1.5, 0.0, 0.5]
+# (name, case, nx, ny, nz, steps, seed, b0[, options]); options: rke (0/1),
+# geometry (0/1/2) and domain [x0, x1, y0, y1, z0, z1]
 CASES = [
     ("ot_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0),
     ("ot_7x5x3_s3", "ot", 7, 5, 3, 3, 1, 0.0),
@@ -37,8 +39,14 @@ CASES = [
     ("harris_10x2x4_s3", "harris", 10, 2, 4, 3, 3, 0.0),
     # the remap kinetic-energy correction on (rke): the reference run on one
     # thread, where its atomic adds happen in loop order
-    ("ot_rke_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0, 1),
-    ("rf_rke_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0, 1),
+    ("ot_rke_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0, {"rke": 1}),
+    ("rf_rke_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0, {"rke": 1}),
+    # cylindrical (1) and spherical (2) geometry on r in [1, 2], theta in
+    # [0.5, 1.5], third coordinate in [0, 0.5]
+    ("ot_cyl_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0, {"geometry": 1, "domain": GEO_DOMAIN}),
+    ("rf_sph_10x8x6_s3", "rf", 10, 8, 6, 3, 7, 0.0, {"geometry": 2, "domain": GEO_DOMAIN}),
+    ("harris_cyl_10x8x4_s3", "harris", 10, 8, 4, 3, 3, 0.0, {"geometry": 1, "domain": GEO_DOMAIN}),
+    ("ot_sph_rke_10x8x6_s4", "ot", 10, 8, 6, 4, 1, 0.0, {"geometry": 2, "domain": GEO_DOMAIN, "rke": 1}),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 # (file, case, nx, ny, nz, steps, seed): the reference's full harness state
@@ -53,17 +61,22 @@ def main():
     if not os.path.exists(lo.REF_BIN):
         raise SystemExit("reference harness not built (needs the reference tree)")
     for name, case, nx, ny, nz, steps, seed, b0, *opt in CASES:
-        rke = opt[0] if opt else 0
+        o = opt[0] if opt else {}
+        rke, geometry, domain = o.get("rke", 0), o.get("geometry", 0), o.get("domain")
+        extra = (["--rke"] if rke else []) + (["--geometry", str(geometry)] if geometry else [])
+        if domain:
+            extra += ["--domain"] + [repr(x) for x in domain]
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "d.dump")
             summary = lo.run_reference(case, nx, ny, nz, steps, path, seed=seed, b0=b0,
-                                       extra=["--rke"] if rke else (), threads=1 if rke else None)
+                                       extra=extra, threads=1 if rke else None)
             d = Dump(path)
             out = {}
             for f in STATE:
                 out[f] = d.box(f)
             out["dts"] = np.array(d.header["dts"])
-            meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0, rke=rke,
+            meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0, rke=rke, geometry=geometry,
+                        domain=domain,
                         time=summary["time"], generator="oracle/_ref/lare_ref (reference LARE3D)")
             out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -87,3 +100,14 @@ def load(name):
 
 if __name__ == "__main__":
     main()
+
+
+def apply_options(p, meta):
+    """Set a case's rke / geometry / domain options (from a fixture's meta) on
+    a parameter block of either ctypes binding."""
+    p.rke = meta.get("rke", 0)
+    p.geometry = meta.get("geometry", 0)
+    d = meta.get("domain")
+    if d:
+        p.x_min, p.x_max, p.y_min, p.y_max, p.z_min, p.z_max = d
+    return p

@@ -46,7 +46,7 @@ def test_abi_version_and_error_string():
 
 def test_create_rejects_bad_params_without_gpu():
     p, b = lare.case_setup("ot", 8, 8, 4)
-    p.geometry = 1
+    p.geometry = 3               # no such geometry (0, 1, 2 are built)
     with pytest.raises(lare.LareError) as e:
         lare.LARE3D(p, b)
     assert e.value.status == -4

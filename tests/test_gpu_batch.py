@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 from sams_b200 import lare
+from tests.golden.make_golden import GEO_DOMAIN, apply_options
 
 pytestmark = pytest.mark.gpu
 
@@ -14,9 +15,11 @@ MIX = [("ot", (16, 12, 4), 1, 0.0), ("ot", (24, 24, 4), 2, 0.9 / (4 * np.pi) ** 
        ("ot", (20, 16, 2), 6, 0.0), ("rf", (10, 2, 8), 7, 0.0)]
 
 
-def _solo(case, n, seed, b0, steps, rke=0):
+def _solo(case, n, seed, b0, steps, rke=0, geometry=0):
     p, b = lare.case_setup(case, *n, b0)
     p.rke = rke
+    if geometry:
+        apply_options(p, {"geometry": geometry, "domain": GEO_DOMAIN})
     s = lare.LARE3D(p, b)
     s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
     s.step(steps)
@@ -26,9 +29,11 @@ def _solo(case, n, seed, b0, steps, rke=0):
     return out, st
 
 
-def _add(batch, case, n, seed, b0, rke=0):
+def _add(batch, case, n, seed, b0, rke=0, geometry=0):
     p, b = lare.case_setup(case, *n, b0)
     p.rke = rke
+    if geometry:
+        apply_options(p, {"geometry": geometry, "domain": GEO_DOMAIN})
     return batch.add(p, b, lare.case_fields(case, p, seed=seed, b0=b0))
 
 
@@ -89,5 +94,19 @@ def test_batch_mixing_rke_and_plain_solves_equals_solo():
     bt.synchronize()
     for sid, (case, n, seed, b0, rke) in zip(ids, mix):
         ref, st = _solo(case, n, seed, b0, 5, rke)
+        _check_equal(bt, sid, case, n, ref, st)
+    bt.close()
+
+
+def test_batch_mixing_geometries_equals_solo():
+    """Cartesian, cylindrical and spherical solves in one batch."""
+    mix = [("ot", (20, 16, 4), 1, 0.0, 0, 1), ("rf", (12, 10, 8), 2, 0.0, 0, 2), ("ot", (16, 12, 4), 3, 0.0, 1, 0),
+           ("harris", (12, 10, 6), 4, 0.0, 0, 1)]
+    bt = lare.Batch()
+    ids = [_add(bt, *m) for m in mix]
+    bt.step(4, graph=True)
+    bt.synchronize()
+    for sid, (case, n, seed, b0, rke, geo) in zip(ids, mix):
+        ref, st = _solo(case, n, seed, b0, 4, rke, geo)
         _check_equal(bt, sid, case, n, ref, st)
     bt.close()

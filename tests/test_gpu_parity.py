@@ -9,14 +9,16 @@ import numpy as np
 import pytest
 
 from sams_b200 import lare
-from tests.golden.make_golden import CASES, STATE, load
+from tests.golden.make_golden import CASES, GEO_DOMAIN, STATE, apply_options, load
 
 pytestmark = pytest.mark.gpu
 
 
-def _solver(case, nx, ny, nz, seed=1, b0=0.0, rke=0):
+def _solver(case, nx, ny, nz, seed=1, b0=0.0, rke=0, options=None):
     p, b = lare.case_setup(case, nx, ny, nz, b0)
     p.rke = rke
+    if options:
+        apply_options(p, options)
     s = lare.LARE3D(p, b)
     s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
     return s
@@ -36,7 +38,7 @@ def _assert_state_equal(s, ref_field, label):
 @pytest.mark.parametrize("name", [c[0] for c in CASES])
 def test_gpu_matches_reference_golden(name):
     z, meta = load(name)
-    s = _solver(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["seed"], meta["b0"], meta.get("rke", 0))
+    s = _solver(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["seed"], meta["b0"], options=meta)
     dts = []
     for _ in range(meta["steps"]):
         s.step(1)
@@ -162,3 +164,22 @@ def test_gpu_resistive_with_inconsistent_energy_ghosts(oracle_lib):
         o.step(1)
         assert s.dt == o.dt
     _assert_state_equal(s, lambda f: _masked(o.field(f), f, *n), "rf ghosts")
+
+
+@pytest.mark.parametrize("case,n,steps,geometry,rke", [("ot", (24, 20, 8), 6, 1, 0), ("rf", (16, 12, 10), 4, 2, 0),
+                                                       ("harris", (16, 12, 6), 4, 1, 1), ("rf", (12, 10, 2), 3, 2, 1)])
+def test_gpu_matches_checker_in_curvilinear_geometry(case, n, steps, geometry, rke, oracle_lib):
+    """Cylindrical and spherical geometry (metric factors on r in [1, 2],
+    theta in [0.5, 1.5]) against the checker, bit for bit."""
+    lo = oracle_lib
+    nx, ny, nz = n
+    opts = {"geometry": geometry, "rke": rke, "domain": GEO_DOMAIN}
+    s = _solver(case, nx, ny, nz, seed=6, options=opts)
+    p, b = lo.case_setup(case, nx, ny, nz)
+    apply_options(p, opts)
+    o = lo.Oracle(p, b, lo.case_fields(case, p, seed=6))
+    for _ in range(steps):
+        s.step(1, graph=True)
+        o.step(1)
+        assert s.dt == o.dt
+    _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"geometry {geometry} {case}{n}")

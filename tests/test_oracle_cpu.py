@@ -11,12 +11,12 @@ import numpy as np
 import pytest
 
 from oracle import lare_oracle as lo
-from tests.golden.make_golden import CASES, STATE, load
+from tests.golden.make_golden import CASES, GEO_DOMAIN, STATE, apply_options, load
 
 
-def _run_checker(case, nx, ny, nz, steps, seed, b0, rke=0):
+def _run_checker(case, nx, ny, nz, steps, seed, b0, options=None):
     p, b = lo.case_setup(case, nx, ny, nz, b0)
-    p.rke = rke
+    apply_options(p, options or {})
     o = lo.Oracle(p, b, lo.case_fields(case, p, seed=seed, b0=b0))
     dts = []
     for _ in range(steps):
@@ -29,7 +29,7 @@ def _run_checker(case, nx, ny, nz, steps, seed, b0, rke=0):
 def test_checker_matches_reference_golden(name, oracle_lib):
     z, meta = load(name)
     o, dts = _run_checker(meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["steps"], meta["seed"], meta["b0"],
-                          meta.get("rke", 0))
+                          meta)
     assert np.array_equal(np.array(dts), z["dts"]), "dt history differs"
     for f in STATE:
         ref = z[f]
@@ -39,19 +39,23 @@ def test_checker_matches_reference_golden(name, oracle_lib):
 
 
 @pytest.mark.skipif(not os.path.exists(lo.REF_BIN), reason="reference harness binary not built here")
-@pytest.mark.parametrize("case,n,steps,rke", [("ot", (9, 11, 5), 12, 0), ("rf", (8, 8, 8), 6, 0),
-                                              ("harris", (10, 8, 4), 6, 0), ("rf", (8, 8, 2), 3, 0),
-                                              ("ot", (2, 9, 5), 3, 0), ("ot", (9, 11, 5), 6, 1),
-                                              ("harris", (10, 8, 4), 4, 1)])
-def test_checker_matches_reference_binary(case, n, steps, rke, tmp_path, oracle_lib):
-    """rke = 1: the reference on one thread (its atomic adds in loop order)."""
+@pytest.mark.parametrize("case,n,steps,rke,geometry", [
+    ("ot", (9, 11, 5), 12, 0, 0), ("rf", (8, 8, 8), 6, 0, 0), ("harris", (10, 8, 4), 6, 0, 0),
+    ("rf", (8, 8, 2), 3, 0, 0), ("ot", (2, 9, 5), 3, 0, 0), ("ot", (9, 11, 5), 6, 1, 0),
+    ("harris", (10, 8, 4), 4, 1, 0), ("ot", (9, 11, 5), 6, 0, 1), ("rf", (8, 6, 6), 3, 0, 2),
+    ("harris", (10, 8, 4), 3, 1, 2)])
+def test_checker_matches_reference_binary(case, n, steps, rke, geometry, tmp_path, oracle_lib):
+    """rke = 1: the reference on one thread (its atomic adds in loop order);
+    geometry 1/2: cylindrical/spherical on r in [1, 2], theta in [0.5, 1.5]."""
     from oracle.dumpio import Dump
     nx, ny, nz = n
     dump = str(tmp_path / "ref.dump")
-    lo.run_reference(case, nx, ny, nz, steps, dump, seed=11, extra=["--rke"] if rke else (),
-                     threads=1 if rke else None)
+    extra = (["--rke"] if rke else []) + (["--geometry", str(geometry), "--domain"] + [repr(x) for x in GEO_DOMAIN]
+                                           if geometry else [])
+    lo.run_reference(case, nx, ny, nz, steps, dump, seed=11, extra=extra, threads=1 if rke else None)
     d = Dump(dump)
-    o, dts = _run_checker(case, nx, ny, nz, steps, 11, 0.0, rke)
+    opts = {"rke": rke, "geometry": geometry, "domain": GEO_DOMAIN if geometry else None}
+    o, dts = _run_checker(case, nx, ny, nz, steps, 11, 0.0, opts)
     assert dts == d.header["dts"]
     for f in lo.FIELD_NAMES:
         ref = d.box(f)
