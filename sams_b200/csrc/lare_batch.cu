@@ -31,7 +31,7 @@ __device__ __forceinline__ void load_ctx(Ctx &dst, const Ctx *src)
 
 // GEO: some solve of the batch is curvilinear (the Cartesian instantiation,
 // used when none is, carries no metric factors).
-template <class Op, bool GEO>
+template <class Op, bool GEO, bool P2>
 __global__ void __launch_bounds__(kT, Op::kMinBlocks)
     kb_op(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int arg, int tile_i,
           int resistive_only)
@@ -52,11 +52,11 @@ __global__ void __launch_bounds__(kT, Op::kMinBlocks)
         const int j = -2 + p / ek, k = -2 + p % ek;
         if (j < lo[1] || j > hi[1] || k < lo[2] || k > hi[2]) continue;
         const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
-        for (int i = ia; i <= ib; ++i) Op::template run<GEO>(c, a, i, j, k);
+        for (int i = ia; i <= ib; ++i) Op::template run<GEO, P2>(c, a, i, j, k);
     }
 }
 
-template <bool GEO>
+template <bool GEO, bool P2>
 __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
     kb_visc(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int tile_i)
 {
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
             if (j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
                 const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
                 for (int i = ia; i <= ib; ++i) {
-                    double cand = ops::Visc::template run<GEO>(c, 0, i, j, k, bad);
+                    double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
                     best = dev::pmin(best, cand);
                 }
             }
@@ -387,6 +387,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     c.gf = GeomF{};
     if (p.geometry) geom_bind(c.gf, s.axes + geo_off, p);
     c.p.geometry = (int)p.geometry;
+    c.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, &c.rc) ? 1 : 0;
     c.p.gamma = p.gas_gamma;
     c.p.mu0 = p.mu0;
     c.p.visc1 = p.visc1;
@@ -473,6 +474,7 @@ int Batch::rebuild()
     has_resistive_ = 0;
     has_rke_ = 0;
     has_geo_ = 0;
+    all_pow2_ = 1;
     for (size_t q = 0; q < slots_.size(); ++q) {
         ctx[q] = slots_[q].ctx;
         bcs[q] = slots_[q].bc;
@@ -483,6 +485,7 @@ int Batch::rebuild()
         has_resistive_ |= slots_[q].ctx.p.resistive;
         has_rke_ |= slots_[q].ctx.p.rke;
         has_geo_ |= slots_[q].ctx.p.geometry != 0;
+        all_pow2_ &= slots_[q].ctx.p.pow2;
         shell_off.push_back(shell);
         const long long e0 = g.nx + 5, e1 = g.ny + 5, e2 = g.nz + 5;
         shell += 5 * e1 * e2 + (long long)g.nx * 5 * e2 + (long long)g.nx * g.ny * 5;
@@ -556,10 +559,13 @@ void Batch::launch(int arg, bool resistive_only)
 {
     if (ntiles_ == 0) return;
     const int grid = std::min(ntiles_, sm_count_ * blocks_per_sm_);
+    const int ro = resistive_only ? 1 : 0;
     if (has_geo_)
-        kb_op<Op, true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, resistive_only ? 1 : 0);
+        kb_op<Op, true, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, ro);
+    else if (all_pow2_)
+        kb_op<Op, false, true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, ro);
     else
-        kb_op<Op, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, resistive_only ? 1 : 0);
+        kb_op<Op, false, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, ro);
 }
 
 void Batch::launch_visc()
@@ -567,9 +573,11 @@ void Batch::launch_visc()
     if (ntiles_ == 0) return;
     const int grid = std::min(ntiles_, sm_count_ * blocks_per_sm_);
     if (has_geo_)
-        kb_visc<true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
+        kb_visc<true, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
+    else if (all_pow2_)
+        kb_visc<false, true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
     else
-        kb_visc<false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
+        kb_visc<false, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, tile_i_);
 }
 
 void Batch::bc_fill(unsigned mask, bool resistive_only)

@@ -101,6 +101,7 @@ private:
     int has_resistive_ = 0;
     int has_rke_ = 0;
     int has_geo_ = 0;
+    int all_pow2_ = 0;  // every live solve has a power-of-two grid
     size_t table_cap_bytes_ = 0;
     std::map<long long, cudaGraphExec_t> graphs_;
 };

@@ -56,6 +56,15 @@ struct Phys {
     int resistive;  // per-solve resistive flag (read by the batched launcher)
     int rke;        // remap kinetic-energy correction on (Ctx::dke allocated)
     int geometry;   // 0 Cartesian, 1 cylindrical, 2 spherical (Ctx::gf set)
+    int pow2;       // Cartesian grid whose spacings are all one power of two each (Ctx::rc set)
+};
+
+// Reciprocals of the spacings and of the cell volume of a uniform Cartesian
+// grid whose spacings are powers of two.  Dividing by a power of two and
+// multiplying by its reciprocal give the same correctly rounded result for
+// every operand, so kernels built for such grids multiply instead.
+struct Recip {
+    double xb, yb, zb, xc, yc, zc, cv;
 };
 
 // Metric factors of a cylindrical or spherical solve, as LARE3D::grid builds
@@ -121,6 +130,7 @@ struct Ctx {
     double *s[NSCRATCH];
     double *dke;  // delta_ke of the rke correction (null unless Phys::rke)
     GeomF gf;     // metric factors (null in Cartesian geometry)
+    Recip rc;     // reciprocals (valid when Phys::pow2)
     Scalars *sc;
 };
 
@@ -136,6 +146,20 @@ struct RO {
     const double *p;
     __device__ __forceinline__ double operator[](int i) const { return __ldg(p + i); }
 };
+
+// x / d, or x * r where the kernel is built for a power-of-two grid (r = 1/d
+// exactly; see Recip).
+template <bool P2>
+__device__ __forceinline__ double div_by(double x, double d, double r)
+{
+    if constexpr (P2) {
+        (void)d;
+        return x * r;
+    } else {
+        (void)r;
+        return x / d;
+    }
+}
 
 // portableWrapper min/max semantics (include/pp/utils.h:277-335).
 __device__ __forceinline__ double pmin(double a, double b) { return a < b ? a : b; }
@@ -255,11 +279,11 @@ __device__ __forceinline__ double mom_flux(double v_advect, double dt, double ar
 
 // Caramana edge viscosity (lagran.cpp:56-93).  v[a] are the four points
 // along the edge direction, o1/o2 the edge ends.
-template <class A>
+template <bool P2, class A>
 __device__ __forceinline__ double edge_viscosity(double dt, double visc1, double v2n, const A &vx,
                                                  const A &vy, const A &vz, const A &rho_v,
                                                  double dvdots, double dx, double dxm, double dxp,
-                                                 double cs_edge, int o0, int o1, int o2, int o3)
+                                                 double cs_edge, int o0, int o1, int o2, int o3, double rdx = 0.0)
 {
     dvdots = pmin(0.0, dvdots);
     double rv1 = rho_v[o1], rv2 = rho_v[o2];
@@ -268,7 +292,7 @@ __device__ __forceinline__ double edge_viscosity(double dt, double visc1, double
     double dvx = vx1 - vx2, dvy = vy1 - vy2, dvz = vz1 - vz2;
     double dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
     double dv = sqrt(dv2);
-    bool small = dv * dt / dx < 1.e-14;
+    bool small = div_by<P2>(dv * dt, dx, rdx) < 1.e-14;
     dvdots = small ? 0.0 : dvdots / dv;
     double dvxm = vx[o0] - vx1, dvxp = vx2 - vx[o3];
     double dvym = vy[o0] - vy1, dvyp = vy2 - vy[o3];

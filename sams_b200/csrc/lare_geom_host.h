@@ -81,4 +81,37 @@ inline void geom_bind(GeomF &gf, const double *dev, const sams_lare_params &p)
     gf.cot = gf.hzc + P;
 }
 
+// True when every spacing array (as the axis builders lay them out: index
+// i + 2, b over -2..n+2, c over -1..n+2) holds one value per axis and that
+// value is a power of two; fills the reciprocals (exact for powers of two).
+inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> &dyb, const std::vector<double> &dzb,
+                      const std::vector<double> &dxc, const std::vector<double> &dyc, const std::vector<double> &dzc,
+                      Recip *rc)
+{
+    auto uniform = [](const std::vector<double> &d, size_t from, size_t to, double *v) {
+        if (d.size() < to || from >= to) return false;
+        const double x = d[from];
+        int e;
+        if (!(x > 0.0) || !(x < DBL_MAX) || std::frexp(x, &e) != 0.5) return false;
+        for (size_t q = from; q < to; ++q)
+            if (d[q] != x) return false;
+        *v = x;
+        return true;
+    };
+    double xb, yb, zb, xc, yc, zc;
+    // b: array indices 0 .. n+4 (i = -2 .. n+2); c: 1 .. n+4 (i = -1 .. n+2)
+    if (!uniform(dxb, 0, dxb.size() - 1, &xb) || !uniform(dyb, 0, dyb.size() - 1, &yb) ||
+        !uniform(dzb, 0, dzb.size() - 1, &zb) || !uniform(dxc, 1, dxc.size() - 1, &xc) ||
+        !uniform(dyc, 1, dyc.size() - 1, &yc) || !uniform(dzc, 1, dzc.size() - 1, &zc))
+        return false;
+    rc->xb = 1.0 / xb;
+    rc->yb = 1.0 / yb;
+    rc->zb = 1.0 / zb;
+    rc->xc = 1.0 / xc;
+    rc->yc = 1.0 / yc;
+    rc->zc = 1.0 / zc;
+    rc->cv = 1.0 / (xb * (yb * zb));
+    return true;
+}
+
 }  // namespace sams

@@ -113,7 +113,7 @@ struct CellPrep {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -144,7 +144,7 @@ struct NodePrep {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -157,11 +157,11 @@ struct NodePrep {
         double sum_rho_cv = rho[o0] * cv0 + rho[o1] * cv1 + rho[o2] * cv2 + rho[o3] * cv3 +
                             rho[o4] * cv4 + rho[o5] * cv5 + rho[o6] * cv6 + rho[o7] * cv7;
         double sum_cv = cv0 + cv1 + cv2 + cv3 + cv4 + cv5 + cv6 + cv7;
-        c.s[S_RHOV][o0] = sum_rho_cv / sum_cv;
+        c.s[S_RHOV][o0] = div_by<P2>(sum_rho_cv, sum_cv, 0.125 * c.rc.cv);
         double cv_v = 0.125 * sum_cv;
         double sum = cs[o0] * cv0 + cs[o1] * cv1 + cs[o2] * cv2 + cs[o3] * cv3 +
                      cs[o4] * cv4 + cs[o5] * cv5 + cs[o6] * cv6 + cs[o7] * cv7;
-        c.s[S_CSV][o0] = 0.125 * sum / cv_v;
+        c.s[S_CSV][o0] = div_by<P2>(0.125 * sum, cv_v, c.rc.cv);
     }
 };
 
@@ -173,7 +173,7 @@ struct Alpha {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -187,7 +187,7 @@ struct Alpha {
             double dx = c.ax.dxb[i + 2], dxp = c.ax.dxb[i + 3], dxm = c.ax.dxb[i + 1];
             double dvdots = -(vx[o1] - vx[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
-            c.s[S_A1][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+            c.s[S_A1][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.xb);
         }
         if (j >= 0 && j <= g.ny + 1) {  // alpha2: (-1..nx+1, 0..ny+1, 0..nz+2)
             int o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
@@ -199,7 +199,7 @@ struct Alpha {
             }
             double dvdots = -(vy[o1] - vy[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
-            c.s[S_A2][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+            c.s[S_A2][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.yb);
         }
         if (j <= g.ny + 1 && k <= g.nz + 1) {  // alpha3: (-1..nx+1, -1..ny+1, 0..nz+1)
             int o1 = o - 1, o2 = o;
@@ -211,7 +211,7 @@ struct Alpha {
             }
             double dvdots = -(vz[o1] - vz[o2]);
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
-            c.s[S_A3][o] = edge_viscosity(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3);
+            c.s[S_A3][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.zb);
         }
     }
 };
@@ -228,7 +228,7 @@ struct Visc {
     // nonfinite is set when a NaN or infinity shows up in this cell's viscous
     // pressure, heating or CFL terms (the solve's state is no longer finite;
     // the min itself would hide it, as LARE's min does).
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
     {
         const Geom &g = c.g;
@@ -274,7 +274,7 @@ struct Visc {
                     - 0.25 * dx * dy * a3a[o - SX - SY] * a11
                     - 0.25 * dx * dy * a3a[o - SY] * a12;
         const double cv = (GEO && c.p.geometry) ? cv_at<GEO>(c, i, j, k) : dx * (dyp * dzp);
-        c.s[S_VH][o] = vh / cv;
+        c.s[S_VH][o] = div_by<P2>(vh, cv, c.rc.cv);
         if (i > g.nx || j > g.ny || k > g.nz) return DBL_MAX;
 
         // viscous forces on node (i, j, k)
@@ -290,8 +290,8 @@ struct Visc {
             double sum_cv = cv_at<GEO>(c, i, j, k) + cv_at<GEO>(c, ip, j, k) + cv_at<GEO>(c, i, jp, k) + cv_at<GEO>(c, ip, jp, k) +
                             cv_at<GEO>(c, i, j, kp) + cv_at<GEO>(c, ip, j, kp) + cv_at<GEO>(c, i, jp, kp) + cv_at<GEO>(c, ip, jp, kp);
             double cv_v = 0.125 * sum_cv;
-#define FV(v) ((e1 * (v[o] - v[o - SX]) + e2 * (v[o] - v[o + SX]) + e3 * (v[o] - v[o - SY]) + \
-                e4 * (v[o] - v[o + SY]) + e5 * (v[o] - v[o - 1]) + e6 * (v[o] - v[o + 1])) / cv_v)
+#define FV(v) div_by<P2>(e1 * (v[o] - v[o - SX]) + e2 * (v[o] - v[o + SX]) + e3 * (v[o] - v[o - SY]) + \
+                e4 * (v[o] - v[o + SY]) + e5 * (v[o] - v[o - 1]) + e6 * (v[o] - v[o + 1]), cv_v, c.rc.cv)
             c.s[S_FXV][o] = FV(vx);
             c.s[S_FYV][o] = FV(vy);
             c.s[S_FZV][o] = FV(vz);
@@ -348,19 +348,20 @@ struct ResistRK {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dxc = c.ax.dxc[i + 2], dyc = c.ax.dyc[j + 2], dzc = c.ax.dzc[k + 2];
-        double jx1 = (bz[o + SY] - bz[o]) / dyc - (by[o + 1] - by[o]) / dzc;
-        double jx2 = (bz[o + SX + SY] - bz[o + SX]) / dyc - (by[o + SX + 1] - by[o + SX]) / dzc;
-        double jy1 = (bx[o + 1] - bx[o]) / dzc - (bz[o + SX] - bz[o]) / dxc;
-        double jy2 = (bx[o + SY + 1] - bx[o + SY]) / dzc - (bz[o + SX + SY] - bz[o + SY]) / dxc;
-        double jz1 = (by[o + SX] - by[o]) / dxc - (bx[o + SY] - bx[o]) / dyc;
-        double jz2 = (by[o + SX + 1] - by[o + 1]) / dxc - (bx[o + SY + 1] - bx[o + 1]) / dyc;
+        const double rx = c.rc.xc, ry = c.rc.yc, rz = c.rc.zc;
+        double jx1 = div_by<P2>(bz[o + SY] - bz[o], dyc, ry) - div_by<P2>(by[o + 1] - by[o], dzc, rz);
+        double jx2 = div_by<P2>(bz[o + SX + SY] - bz[o + SX], dyc, ry) - div_by<P2>(by[o + SX + 1] - by[o + SX], dzc, rz);
+        double jy1 = div_by<P2>(bx[o + 1] - bx[o], dzc, rz) - div_by<P2>(bz[o + SX] - bz[o], dxc, rx);
+        double jy2 = div_by<P2>(bx[o + SY + 1] - bx[o + SY], dzc, rz) - div_by<P2>(bz[o + SX + SY] - bz[o + SY], dxc, rx);
+        double jz1 = div_by<P2>(by[o + SX] - by[o], dxc, rx) - div_by<P2>(bx[o + SY] - bx[o], dyc, ry);
+        double jz2 = div_by<P2>(by[o + SX + 1] - by[o + 1], dxc, rx) - div_by<P2>(bx[o + SY + 1] - bx[o + 1], dyc, ry);
         double jx = 0.5 * (jx1 + jx2), jy = 0.5 * (jy1 + jy2), jz = 0.5 * (jz1 + jz2);
         double j_local = sqrt(jx * jx + jy * jy + jz * jz);
         double eta = j_local > c.p.j_max ? c.p.eta_bg + c.p.eta0 : c.p.eta_bg;
@@ -380,7 +381,7 @@ struct ResistB {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int last, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -398,15 +399,15 @@ struct ResistB {
         const bool inx1 = i >= 1 && i <= g.nx, iny1 = j >= 1 && j <= g.ny, inz1 = k >= 1 && k <= g.nz;
         if (inx && iny1 && inz1) {
             double area = c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
-            bx[o] = bxo + (fz[o] - fz[o - SY] + fz[o - 1] - fz[o - SY - 1] - fy[o] + fy[o - 1] - fy[o - SY] + fy[o - SY - 1]) * dt / area;
+            bx[o] = bxo + div_by<P2>((fz[o] - fz[o - SY] + fz[o - 1] - fz[o - SY - 1] - fy[o] + fy[o - 1] - fy[o - SY] + fy[o - SY - 1]) * dt, area, c.rc.yb * c.rc.zb);
         }
         if (inx1 && iny && inz1) {
             double area = c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
-            by[o] = byo + (fx[o] - fx[o - 1] + fx[o - SX] - fx[o - SX - 1] - fz[o] + fz[o - SX] - fz[o - 1] + fz[o - SX - 1]) * dt / area;
+            by[o] = byo + div_by<P2>((fx[o] - fx[o - 1] + fx[o - SX] - fx[o - SX - 1] - fz[o] + fz[o - SX] - fz[o - 1] + fz[o - SX - 1]) * dt, area, c.rc.xb * c.rc.zb);
         }
         if (inx1 && iny1 && inz) {
             double area = c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
-            bz[o] = bzo + (fy[o] - fy[o - SX] + fy[o - SY] - fy[o - SX - SY] - fx[o] + fx[o - SY] - fx[o - SX] + fx[o - SX - SY]) * dt / area;
+            bz[o] = bzo + div_by<P2>((fy[o] - fy[o - SX] + fy[o - SY] - fy[o - SX - SY] - fx[o] + fx[o - SY] - fx[o - SX] + fx[o - SX - SY]) * dt, area, c.rc.xb * c.rc.yb);
         }
         if (inx1 && iny1 && inz1) {
             const RO curlb{c.s[S_CURLB]};
@@ -426,7 +427,7 @@ struct Pred1 {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -444,9 +445,9 @@ struct Pred1 {
         double vzb = 0.25 * (vz[a] + vz[am] + vz[bm] + vz[am - SY]);
         double vzbm = 0.25 * (vz[cm] + vz[am - 1] + vz[bm - 1] + vz[am - SY - 1]);
         double vol = cv_at<GEO>(c, i, j, k);
-        double dvxdx = (vxb * dxab0 - vxbm * dxabm) / vol;
-        double dvydy = (vyb * dyab0 - vybm * dyabm) / vol;
-        double dvzdz = (vzb * dzab0 - vzbm * dzabm) / vol;
+        double dvxdx = div_by<P2>(vxb * dxab0 - vxbm * dxabm, vol, c.rc.cv);
+        double dvydy = div_by<P2>(vyb * dyab0 - vybm * dyabm, vol, c.rc.cv);
+        double dvzdz = div_by<P2>(vzb * dzab0 - vzbm * dzabm, vol, c.rc.cv);
         double dv = (dvxdx + dvydy + dvzdz) * dt / 2.0;
         double cv1 = vol * (1.0 + dv);
 
@@ -454,22 +455,22 @@ struct Pred1 {
         vxbm = 0.25 * (vx[bm] + vx[bm - SX] + vx[bm - 1] + vx[bm - SX - 1]);
         vyb = 0.25 * (vy[a] + vy[bm] + vy[cm] + vy[bm - 1]);
         vybm = 0.25 * (vy[am] + vy[am - SY] + vy[am - 1] + vy[am - SY - 1]);
-        double dvxdy = (vxb * dyab0 - vxbm * dyabm) / vol;
-        double dvydx = (vyb * dxab0 - vybm * dxabm) / vol;
+        double dvxdy = div_by<P2>(vxb * dyab0 - vxbm * dyabm, vol, c.rc.cv);
+        double dvydx = div_by<P2>(vyb * dxab0 - vybm * dxabm, vol, c.rc.cv);
 
         vxb = 0.25 * (vx[a] + vx[am] + vx[bm] + vx[am - SY]);
         vxbm = 0.25 * (vx[cm] + vx[am - 1] + vx[bm - 1] + vx[am - SY - 1]);
         double vzb2 = 0.25 * (vz[a] + vz[bm] + vz[cm] + vz[bm - 1]);
         double vzbm2 = 0.25 * (vz[am] + vz[am - SY] + vz[am - 1] + vz[am - SY - 1]);
-        double dvxdz = (vxb * dzab0 - vxbm * dzabm) / vol;
-        double dvzdx = (vzb2 * dxab0 - vzbm2 * dxabm) / vol;
+        double dvxdz = div_by<P2>(vxb * dzab0 - vxbm * dzabm, vol, c.rc.cv);
+        double dvzdx = div_by<P2>(vzb2 * dxab0 - vzbm2 * dxabm, vol, c.rc.cv);
 
         vyb = 0.25 * (vy[a] + vy[am] + vy[bm] + vy[am - SY]);
         vybm = 0.25 * (vy[cm] + vy[am - 1] + vy[bm - 1] + vy[am - SY - 1]);
         vzb2 = 0.25 * (vz[a] + vz[am] + vz[cm] + vz[am - 1]);
         vzbm2 = 0.25 * (vz[bm] + vz[bm - SX] + vz[bm - 1] + vz[bm - SX - 1]);
-        double dvydz = (vyb * dzab0 - vybm * dzabm) / vol;
-        double dvzdy = (vzb2 * dyab0 - vzbm2 * dyabm) / vol;
+        double dvydz = div_by<P2>(vyb * dzab0 - vybm * dzabm, vol, c.rc.cv);
+        double dvzdy = div_by<P2>(vzb2 * dyab0 - vzbm2 * dyabm, vol, c.rc.cv);
 
         double b1x, b1y, b1z;
         if (resistive) {
@@ -499,7 +500,7 @@ struct Pred1 {
         double ei = __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double pe = resistive ? c.s[S_PE][o] : (gm - 1.0) * rho * ee;
         double pi = resistive ? c.s[S_PI][o] : (gm - 1.0) * rho * ei;
-        double dvv = cv1 / vol - 1.0;
+        double dvv = div_by<P2>(cv1, vol, c.rc.cv) - 1.0;
         double e1_e = ee - pe * dvv / rho;
         double e1_i = ei - pi * dvv / rho;
         e1_i += __ldg(c.s[S_VH] + o) * dt / 2.0 / rho;
@@ -516,7 +517,7 @@ struct Pred2 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -543,13 +544,13 @@ struct Pred2 {
         double ppxy = pe[qxy] + pi[qxy], ppxz = pe[qxz] + pi[qxz], ppyz = pe[qyz] + pi[qyz], ppxyz = pe[qxyz] + pi[qxyz];
         double w1 = pp + ppy + ppz + ppyz;
         double w2 = ppx + ppxy + ppxz + ppxyz;
-        double fx = (w1 - w2) * 0.25 / dx;
+        double fx = div_by<P2>((w1 - w2) * 0.25, dx, c.rc.xc);
         w1 = pp + ppx + ppz + ppxz;
         w2 = ppy + ppxy + ppyz + ppxyz;
-        double fy = (w1 - w2) * 0.25 / dhy;
+        double fy = div_by<P2>((w1 - w2) * 0.25, dhy, c.rc.yc);
         w1 = pp + ppx + ppy + ppxy;
         w2 = ppz + ppxz + ppyz + ppxyz;
-        double fz = (w1 - w2) * 0.25 / dhz;
+        double fz = div_by<P2>((w1 - w2) * 0.25, dhz, c.rc.zc);
 
         double cvx = cv1[q0] + cv1[qy] + cv1[qz] + cv1[qyz];
         double cvxp = cv1[qx] + cv1[qxy] + cv1[qxz] + cv1[qxyz];
@@ -566,11 +567,11 @@ struct Pred2 {
         } else {
             w1 = (bz1[q0] + bz1[qx] + bz1[qz] + bz1[qxz]) / cvy;
             w2 = (bz1[qy] + bz1[qxy] + bz1[qyz] + bz1[qxyz]) / cvyp;
-            jx = (w2 - w1) / dhy;
+            jx = div_by<P2>(w2 - w1, dhy, c.rc.yc);
         }
         w1 = (by1[q0] + by1[qx] + by1[qy] + by1[qxy]) / cvz;
         w2 = (by1[qz] + by1[qxz] + by1[qyz] + by1[qxyz]) / cvzp;
-        jx -= (w2 - w1) / dhz;
+        jx -= div_by<P2>(w2 - w1, dhz, c.rc.zc);
 
         double jy;
         if (geo) {
@@ -580,11 +581,11 @@ struct Pred2 {
         } else {
             w1 = (bz1[q0] + bz1[qy] + bz1[qz] + bz1[qyz]) / cvx;
             w2 = (bz1[qx] + bz1[qxy] + bz1[qxz] + bz1[qxyz]) / cvxp;
-            jy = -(w2 - w1) / dx;
+            jy = div_by<P2>(-(w2 - w1), dx, c.rc.xc);
         }
         w1 = (bx1[q0] + bx1[qx] + bx1[qy] + bx1[qxy]) / cvz;
         w2 = (bx1[qz] + bx1[qxz] + bx1[qyz] + bx1[qxyz]) / cvzp;
-        jy += (w2 - w1) / dhz;
+        jy += div_by<P2>(w2 - w1, dhz, c.rc.zc);
 
         double jz;
         if (geo) {
@@ -594,11 +595,11 @@ struct Pred2 {
         } else {
             w1 = (by1[q0] + by1[qy] + by1[qz] + by1[qyz]) / cvx;
             w2 = (by1[qx] + by1[qxy] + by1[qxz] + by1[qxyz]) / cvxp;
-            jz = (w2 - w1) / dx;
+            jz = div_by<P2>(w2 - w1, dx, c.rc.xc);
         }
         w1 = (bx1[q0] + bx1[qx] + bx1[qz] + bx1[qxz]) / cvy;
         w2 = (bx1[qy] + bx1[qxy] + bx1[qyz] + bx1[qxyz]) / cvyp;
-        jz -= (w2 - w1) / dhy;
+        jz -= div_by<P2>(w2 - w1, dhy, c.rc.yc);
 
 #define SUM8(a) (a[q0] + a[qx] + a[qy] + a[qxy] + a[qz] + a[qxz] + a[qyz] + a[qxyz])
         double bxv = SUM8(bx1) / (cvx + cvxp);
@@ -641,7 +642,7 @@ struct Corr1 {
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -675,7 +676,7 @@ struct Corr1 {
                      0.25 * dx * dz * a2a[o - SX] * a4 - 0.25 * dy * dz * a1a[o + 1] * a5 - 0.25 * dx * dz * a2a[o + 1] * a6 -
                      0.25 * dy * dz * a1a[o + SY + 1] * a7 - 0.25 * dx * dz * a2a[o - SX + 1] * a8 - 0.25 * dy * dy * a3a[o] * a9 -
                      0.25 * dx * dy * a3a[o - SX] * a10 - 0.25 * dy * dy * a3a[o - SX - SY] * a11 - 0.25 * dx * dy * a3a[o - SY] * a12);
-        c.s[S_VH][o] = pmax(vh / cv_at<GEO>(c, i, j, k), 0.0);
+        c.s[S_VH][o] = pmax(div_by<P2>(vh, cv_at<GEO>(c, i, j, k), c.rc.cv), 0.0);
     }
 };
 
@@ -688,7 +689,7 @@ struct Corr2 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -711,9 +712,9 @@ struct Corr2 {
         double vzb = 0.25 * (vz1[a] + vz1[am] + vz1[bm] + vz1[am - SY]);
         double vzbm = 0.25 * (vz1[cm] + vz1[am - 1] + vz1[bm - 1] + vz1[am - SY - 1]);
         double vol = cv_at<GEO>(c, i, j, k);
-        double dvxdx = (vxb * dxab_at<GEO>(c, i, j, k) - vxbm * dxab_at<GEO>(c, i - 1, j, k)) / vol;
-        double dvydy = (vyb * dyab_at<GEO>(c, i, j, k) - vybm * dyab_at<GEO>(c, i, j - 1, k)) / vol;
-        double dvzdz = (vzb * dzab_at<GEO>(c, i, j, k) - vzbm * dzab_at<GEO>(c, i, j, k - 1)) / vol;
+        double dvxdx = div_by<P2>(vxb * dxab_at<GEO>(c, i, j, k) - vxbm * dxab_at<GEO>(c, i - 1, j, k), vol, c.rc.cv);
+        double dvydy = div_by<P2>(vyb * dyab_at<GEO>(c, i, j, k) - vybm * dyab_at<GEO>(c, i, j - 1, k), vol, c.rc.cv);
+        double dvzdz = div_by<P2>(vzb * dzab_at<GEO>(c, i, j, k) - vzbm * dzab_at<GEO>(c, i, j, k - 1), vol, c.rc.cv);
         double dv = (dvxdx + dvydy + dvzdz) * dt;
         double *rho = c.f[SAMS_F_RHO], *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
         double r = rho[o];
@@ -735,7 +736,7 @@ struct BScale {
     {
         set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int back, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -775,7 +776,7 @@ struct SweepVol {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -805,20 +806,20 @@ struct SweepVol {
         }
         double dv, cv2, db1;
         if (DIR == 0) {
-            double dvxdx = tx / vol, dvydy = 1.0 * ty / vol, dvzdz = 1.0 * tz / vol;
+            double dvxdx = div_by<P2>(tx, vol, c.rc.cv), dvydy = div_by<P2>(1.0 * ty, vol, c.rc.cv), dvzdz = div_by<P2>(1.0 * tz, vol, c.rc.cv);
             dv = (dvydy + dvzdz) * dt;
             cv2 = vol * (1.0 + dv);
             dv = dv + dvxdx * dt;
             db1 = dxb0 + (vxb - vxbm) * dt;
         } else if (DIR == 1) {
-            double dvydy = ty / vol, dvzdz = 1.0 * tz / vol;
+            double dvydy = div_by<P2>(ty, vol, c.rc.cv), dvzdz = div_by<P2>(1.0 * tz, vol, c.rc.cv);
             dv = dvzdz * dt;
             cv2 = vol * (1.0 + dv);
             dv = dv + dvydy * dt;
             // hyc * dyb (yremap.cpp:78); hyc = 1 in Cartesian geometry
             db1 = ((GEO && c.p.geometry) ? c.gf.hyc[i + 2] * dyb0 : dyb0) + (vyb - vybm) * dt;
         } else {
-            double dvzdz = tz / vol;
+            double dvzdz = div_by<P2>(tz, vol, c.rc.cv);
             dv = 0.0 * dt;
             cv2 = vol * (1.0 + dv);
             dv = dv + dvzdz * dt;
@@ -839,7 +840,7 @@ struct SweepCvc {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 1, -1, g.nz + 1);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -858,7 +859,7 @@ struct SweepCT {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -908,7 +909,7 @@ struct SweepCTUpd {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -974,7 +975,7 @@ struct SweepMass {
         set_bounds(lo, hi, 0, DIR == 0 ? g.nx : g.nx + 1, 0, DIR == 1 ? g.ny : g.ny + 1, 0,
                    DIR == 2 ? g.nz : g.nz + 1);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -1005,7 +1006,7 @@ struct SweepS6 {
         set_bounds(lo, hi, DIR == 0 ? -2 : 0, DIR == 0 ? g.nx + 1 : g.nx, DIR == 1 ? -2 : 0,
                    DIR == 1 ? g.ny + 1 : g.ny, DIR == 2 ? -2 : 0, DIR == 2 ? g.nz + 1 : g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -1062,7 +1063,7 @@ struct SweepS7 {
     {
         set_bounds(lo, hi, DIR == 0 ? -1 : 0, g.nx, DIR == 1 ? -1 : 0, g.ny, DIR == 2 ? -1 : 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -1108,7 +1109,7 @@ struct SweepS8 {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
@@ -1144,7 +1145,7 @@ struct RkeZero {
     {
         set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (c.p.rke) c.dke[box_off(c.g, i, j, k)] = 0.0;
@@ -1164,7 +1165,7 @@ struct SweepRkeDk {
         set_bounds(lo, hi, 0, DIR == 0 ? g.nx - 1 : g.nx, 0, DIR == 1 ? g.ny - 1 : g.ny, 0,
                    DIR == 2 ? g.nz - 1 : g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;
@@ -1204,7 +1205,7 @@ struct SweepRkeGather {
         set_bounds(lo, hi, DIR == 0 ? 1 : 0, DIR == 0 ? g.nx : g.nx + 1, DIR == 1 ? 1 : 0,
                    DIR == 1 ? g.ny : g.ny + 1, DIR == 2 ? 1 : 0, DIR == 2 ? g.nz : g.nz + 1);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;
@@ -1244,7 +1245,7 @@ struct RkeEnergy {
     {
         set_bounds(lo, hi, 1, g.nx, 1, g.ny, 1, g.nz);
     }
-    template <bool GEO>
+    template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         if (!c.p.rke) return;

@@ -31,7 +31,7 @@ constexpr int kThreads = 256;
 // One thread per (j, k) of a plane, blockIdx.y walks i.  GEO: the solve's
 // geometry is curvilinear (its metric factors are applied); the Cartesian
 // instantiation has no trace of them.
-template <class Op, bool GEO>
+template <class Op, bool GEO, bool P2>
 __global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
 {
     int lo[3], hi[3];
@@ -42,13 +42,13 @@ __global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
     if (t >= plane) return;
     const int j = lo[1] + (int)(t / nk);
     const int k = lo[2] + (int)(t % nk);
-    for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::template run<GEO>(c, arg, i, j, k);
+    for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::template run<GEO, P2>(c, arg, i, j, k);
 }
 
 // Visc with the CFL minimum: each block reduces its candidates and folds
 // them into Scalars::dtmin_bits.  Positive doubles order like their bit
 // patterns, so an integer atomicMin is an exact, order-free minimum.
-template <bool GEO>
+template <bool GEO, bool P2>
 __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
 {
     int lo[3], hi[3];
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
         const int j = lo[1] + (int)(t / nk);
         const int k = lo[2] + (int)(t % nk);
         for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) {
-            double cand = ops::Visc::template run<GEO>(c, 0, i, j, k, bad);
+            double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
             best = dev::pmin(best, cand);
         }
     }
@@ -327,6 +327,7 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
     ctx_.gf = GeomF{};
     if (p.geometry) geom_bind(ctx_.gf, axes_ + geo_off, p);
     ctx_.p.geometry = (int)p.geometry;
+    ctx_.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, &ctx_.rc) ? 1 : 0;
 
     ctx_.p.gamma = p.gas_gamma;
     ctx_.p.mu0 = p.mu0;
@@ -469,10 +470,12 @@ void Solver::launch(int arg)
     Op::bounds(ctx_.g, arg, lo, hi);
     const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
     dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(hi[0] - lo[0] + 1));
-    if (p_.geometry)
-        k_op<Op, true><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+    if (ctx_.p.geometry)
+        k_op<Op, true, false><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+    else if (ctx_.p.pow2)
+        k_op<Op, false, true><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
     else
-        k_op<Op, false><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
+        k_op<Op, false, false><<<grid, kThreads, 0, stream_>>>(ctx_, arg);
     ++launches_;
 }
 
@@ -538,10 +541,12 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
         const int ni = hi[0] - lo[0] + 1;
         dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(ni < 16 ? ni : 16));
-        if (p_.geometry)
-            k_visc<true><<<grid, kThreads, 0, stream_>>>(ctx_);
+        if (ctx_.p.geometry)
+            k_visc<true, false><<<grid, kThreads, 0, stream_>>>(ctx_);
+        else if (ctx_.p.pow2)
+            k_visc<false, true><<<grid, kThreads, 0, stream_>>>(ctx_);
         else
-            k_visc<false><<<grid, kThreads, 0, stream_>>>(ctx_);
+            k_visc<false, false><<<grid, kThreads, 0, stream_>>>(ctx_);
         ++launches_;
     }
     k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);

@@ -6,7 +6,7 @@ stores, per case, the nine state fields over their own index ranges plus the
 dt history.  The reference tree is needed only to (re)generate; the .npz
 files are committed and used by tests on machines without it.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]
 """
 import json
 import os
@@ -47,6 +47,11 @@ CASES = [
     ("rf_sph_10x8x6_s3", "rf", 10, 8, 6, 3, 7, 0.0, {"geometry": 2, "domain": GEO_DOMAIN}),
     ("harris_cyl_10x8x4_s3", "harris", 10, 8, 4, 3, 3, 0.0, {"geometry": 1, "domain": GEO_DOMAIN}),
     ("ot_sph_rke_10x8x6_s4", "ot", 10, 8, 6, 4, 1, 0.0, {"geometry": 2, "domain": GEO_DOMAIN, "rke": 1}),
+    # Cartesian grids whose spacings are all one power of two (1/16, 1/8, 1,
+    # 1/2): the GPU divides by multiplying with exact reciprocals there
+    ("ot_p2_16x8x4_s4", "ot", 16, 8, 4, 4, 1, 0.0),
+    ("rf_p2_rke_16x8x8_s4", "rf", 16, 8, 8, 4, 7, 0.0, {"rke": 1}),
+    ("harris_p2_16x8x4_s3", "harris", 16, 8, 4, 3, 3, 0.0, {"domain": [-8.0, 8.0, -4.0, 4.0, 0.0, 2.0]}),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 # (file, case, nx, ny, nz, steps, seed): the reference's full harness state
@@ -56,11 +61,14 @@ RESTARTS = [("ot_12x10x6_at3.dump", "ot", 12, 10, 6, 3, 1)]
 HARNESS = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "vx1", "vy1", "vz1", "bx", "by", "bz", "dm"]
 
 
-def main():
+def main(only=()):
+    """Regenerate every fixture, or only the cases named in `only`."""
     lo.build()
     if not os.path.exists(lo.REF_BIN):
         raise SystemExit("reference harness not built (needs the reference tree)")
     for name, case, nx, ny, nz, steps, seed, b0, *opt in CASES:
+        if only and name not in only:
+            continue
         o = opt[0] if opt else {}
         rke, geometry, domain = o.get("rke", 0), o.get("geometry", 0), o.get("domain")
         extra = (["--rke"] if rke else []) + (["--geometry", str(geometry)] if geometry else [])
@@ -82,6 +90,8 @@ def main():
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
             print(name, "dt", d.header["dt"])
     for fname, case, nx, ny, nz, steps, seed in RESTARTS:
+        if only and fname not in only:
+            continue
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "d.dump")
             lo.run_reference(case, nx, ny, nz, steps, path, seed=seed)
@@ -99,7 +109,7 @@ def load(name):
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))
 
 
 def apply_options(p, meta):
