@@ -187,6 +187,11 @@ typedef struct sams_lare_serve_stats {
     double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> result on host */
     double cell_updates, wall_s, cell_updates_per_s;      /* since creation */
     int64_t device_bytes_in_use;
+    /* outstanding work: interior cells x steps still to run, summed over the
+     * queued and running requests, and the device bytes the queued ones will
+     * take when admitted */
+    double pending_cell_updates;
+    int64_t queued_bytes;
 } sams_lare_serve_stats;
 
 int sams_lare_serve_create(int device, int64_t budget_bytes, sams_lare_server **out);
@@ -199,6 +204,9 @@ int sams_lare_serve_create(int device, int64_t budget_bytes, sams_lare_server **
 int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *params,
                            const sams_lare_bcs *bcs, const double *const ic[SAMS_NFIELDS],
                            int64_t nsteps, double *const out[9], int64_t *ticket);
+/* Device bytes a solve takes while a server runs it (what admission charges
+ * against the budget). */
+int sams_lare_serve_solve_bytes(const sams_lare_params *params, int64_t *bytes);
 /* Cap the interior cells (nx*ny*nz summed) of the solves running at once;
  * 0 (the default) leaves only the memory budget.  Under a backlog a smaller
  * running set finishes each solve sooner, so a cap just large enough to keep
@@ -222,6 +230,44 @@ int sams_lare_serve_drain(sams_lare_server *s, double timeout_s);
 int sams_lare_serve_get_stats(sams_lare_server *s, sams_lare_serve_stats *stats);
 /* Stop the scheduler and free everything. */
 int sams_lare_serve_destroy(sams_lare_server *s);
+
+/* ---- Serving on several GPUs --------------------------------------------
+ * No counterpart in the reference (its runner is one solve per MPI job).
+ * Independent solves need no exchange, so a host router owns one server per
+ * listed device (each with its own scheduler thread, stream and budget) and
+ * sends each submitted solve to the least-loaded one: among the devices
+ * whose budget can hold the solve, those where it fits next to what is
+ * already admitted or queued come first, then the least outstanding work
+ * (pending_cell_updates), then the fewest committed bytes, then the lowest
+ * index.  A device may be listed more than once (two servers share it).
+ * Tickets are the router's own; every call mirrors its sams_lare_serve_*
+ * counterpart. */
+typedef struct sams_lare_router sams_lare_router;
+
+int sams_lare_router_create(const int *devices, int ndevices, int64_t budget_bytes_per_device,
+                            sams_lare_router **out);
+int sams_lare_router_submit(sams_lare_router *r, const sams_lare_params *params,
+                            const sams_lare_bcs *bcs, const double *const ic[SAMS_NFIELDS],
+                            int64_t nsteps, double *const out[9], int64_t *ticket);
+/* Index (into the create call's device list) of the server a ticket went to. */
+int sams_lare_router_placement(sams_lare_router *r, int64_t ticket, int *index);
+int sams_lare_router_set_max_cells(sams_lare_router *r, int64_t max_cells_per_device);
+int sams_lare_router_poll(sams_lare_router *r, int64_t ticket, int *status, double *latency_s);
+int sams_lare_router_fetch(sams_lare_router *r, int64_t ticket, int state_index, double *host_box);
+int sams_lare_router_cancel(sams_lare_router *r, int64_t ticket);
+int sams_lare_router_release(sams_lare_router *r, int64_t ticket);
+int sams_lare_router_drain(sams_lare_router *r, double timeout_s);
+/* Totals over every server; latency percentiles over all completed requests. */
+int sams_lare_router_get_stats(sams_lare_router *r, sams_lare_serve_stats *stats);
+/* One server's own statistics (index into the device list). */
+int sams_lare_router_server_stats(sams_lare_router *r, int index, sams_lare_serve_stats *stats);
+int sams_lare_router_destroy(sams_lare_router *r);
+
+/* The router's placement rule on its own (host only, no device): loads of n
+ * servers, a solve of request_bytes; *index receives the choice.  Returns
+ * SAMS_ERR_BUDGET when no server's budget can hold the solve. */
+int sams_lare_route_pick(int n, const double *pending_cell_updates, const int64_t *committed_bytes,
+                         const int64_t *budget_bytes, int64_t request_bytes, int *index);
 
 /* No counterpart in the reference.  Advance nsteps timesteps of a solve whose
  * 13 fields live in the caller's own device memory, allocating nothing: for

@@ -196,9 +196,9 @@ void sams_lare_server::loop()
         }
         std::vector<Request *> keep;
         for (Request *r : running) {
-            r->done += 1;
             {
                 std::lock_guard<std::mutex> lk(mu);
+                r->done += 1;
                 cell_updates += (double)r->p.nx * (double)r->p.ny * (double)r->p.nz;
             }
             bool finished = r->done >= r->nsteps;
@@ -284,6 +284,13 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
     s->queue.push_back(r.get());
     s->all.emplace(r->id, std::move(r));
     s->cv.notify_all();
+    return SAMS_OK;
+}
+
+int sams_lare_serve_solve_bytes(const sams_lare_params *p, int64_t *bytes)
+{
+    if (!p || !bytes) return SAMS_ERR_INVALID;
+    *bytes = (int64_t)sams::Batch::bytes_for(*p);
     return SAMS_OK;
 }
 
@@ -404,6 +411,15 @@ int sams_lare_serve_get_stats(sams_lare_server *s, sams_lare_serve_stats *st)
     st->wall_s = std::chrono::duration<double>(Clock::now() - s->t_start).count();
     st->cell_updates_per_s = st->wall_s > 0 ? st->cell_updates / st->wall_s : 0.0;
     st->device_bytes_in_use = s->in_use;
+    double pending = 0.0;
+    int64_t qbytes = 0;
+    for (const Request *r : s->queue) {
+        pending += (double)r->cells * (double)r->nsteps;
+        qbytes += r->bytes;
+    }
+    for (const Request *r : s->running) pending += (double)r->cells * (double)(r->nsteps - r->done);
+    st->pending_cell_updates = pending;
+    st->queued_bytes = qbytes;
     return SAMS_OK;
 }
 

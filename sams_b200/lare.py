@@ -368,7 +368,8 @@ class ServeStats(ctypes.Structure):
                 ("p50_latency_s", ctypes.c_double), ("p99_latency_s", ctypes.c_double),
                 ("mean_latency_s", ctypes.c_double), ("cell_updates", ctypes.c_double),
                 ("wall_s", ctypes.c_double), ("cell_updates_per_s", ctypes.c_double),
-                ("device_bytes_in_use", ctypes.c_int64)]
+                ("device_bytes_in_use", ctypes.c_int64), ("pending_cell_updates", ctypes.c_double),
+                ("queued_bytes", ctypes.c_int64)]
 
 
 SERVE_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
@@ -389,7 +390,40 @@ def _bind_serve(L):
     L.sams_lare_serve_drain.argtypes = [vp, ctypes.c_double]
     L.sams_lare_serve_get_stats.argtypes = [vp, ctypes.POINTER(ServeStats)]
     L.sams_lare_serve_destroy.argtypes = [vp]
+    L.sams_lare_serve_solve_bytes.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(i64)]
+    L.sams_lare_router_create.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int, i64, ctypes.POINTER(vp)]
+    L.sams_lare_router_submit.argtypes = L.sams_lare_serve_submit.argtypes
+    L.sams_lare_router_placement.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_int)]
+    for name in ("set_max_cells", "poll", "fetch", "release", "cancel", "drain", "get_stats", "destroy"):
+        getattr(L, "sams_lare_router_" + name).argtypes = getattr(L, "sams_lare_serve_" + name).argtypes
+    L.sams_lare_router_server_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ServeStats)]
+    L.sams_lare_route_pick.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64),
+                                       ctypes.POINTER(i64), i64, ctypes.POINTER(ctypes.c_int)]
     L._serve_bound = True
+
+
+def solve_bytes(params):
+    """Device bytes one solve takes while a server runs it."""
+    L = lib()
+    _bind_serve(L)
+    v = ctypes.c_int64()
+    _check(L.sams_lare_serve_solve_bytes(ctypes.byref(params), ctypes.byref(v)))
+    return v.value
+
+
+def route_pick(pending_cell_updates, committed_bytes, budget_bytes, request_bytes):
+    """The multi-GPU router's placement rule (host only): index of the server
+    a solve of `request_bytes` goes to, given each server's outstanding work
+    and committed bytes."""
+    L = lib()
+    _bind_serve(L)
+    n = len(pending_cell_updates)
+    pend = (ctypes.c_double * n)(*pending_cell_updates)
+    comm = (ctypes.c_int64 * n)(*committed_bytes)
+    bud = (ctypes.c_int64 * n)(*budget_bytes)
+    idx = ctypes.c_int(-1)
+    _check(L.sams_lare_route_pick(n, pend, comm, bud, int(request_bytes), ctypes.byref(idx)))
+    return idx.value
 
 
 class Server:
@@ -397,6 +431,8 @@ class Server:
     serving section).  Submitted solves are admitted as device memory within
     `budget_bytes` frees up, stepped together with every other running solve,
     and their final state copied back when their step count is reached."""
+
+    _prefix = "sams_lare_serve_"
 
     def __init__(self, budget_bytes, device=0, max_cells=0):
         L = lib()
@@ -408,13 +444,16 @@ class Server:
         if max_cells:
             self.set_max_cells(max_cells)
 
+    def _fn(self, name):
+        return getattr(lib(), self._prefix + name)
+
     def set_max_cells(self, max_cells):
         """Cap the interior cells of the solves running at once (0 = none)."""
-        _check(lib().sams_lare_serve_set_max_cells(self._h, int(max_cells)))
+        _check(self._fn("set_max_cells")(self._h, int(max_cells)))
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().sams_lare_serve_destroy(self._h)
+            self._fn("destroy")(self._h)
             self._h = None
 
     def __del__(self):
@@ -430,34 +469,65 @@ class Server:
         if out is not None:
             op = (_P * 9)(*[a.ctypes.data_as(_P) for a in out])
         t = ctypes.c_int64()
-        _check(lib().sams_lare_serve_submit(self._h, ctypes.byref(params), ctypes.byref(bcs), ip, int(nsteps),
+        _check(self._fn("submit")(self._h, ctypes.byref(params), ctypes.byref(bcs), ip, int(nsteps),
                                             op, ctypes.byref(t)))
         self._keep[t.value] = (ic, out, box_shape(params.nx, params.ny, params.nz))
         return t.value
 
     def poll(self, ticket):
         st, lat = ctypes.c_int(), ctypes.c_double()
-        _check(lib().sams_lare_serve_poll(self._h, ticket, ctypes.byref(st), ctypes.byref(lat)))
+        _check(self._fn("poll")(self._h, ticket, ctypes.byref(st), ctypes.byref(lat)))
         return SERVE_STATUS[st.value], lat.value
 
     def fetch(self, ticket, index):
         out = np.empty(self._keep[ticket][2])
-        _check(lib().sams_lare_serve_fetch(self._h, ticket, index, out.ctypes.data_as(_P)))
+        _check(self._fn("fetch")(self._h, ticket, index, out.ctypes.data_as(_P)))
         return out
 
     def cancel(self, ticket):
         """Withdraw a queued or running request (its status becomes
         "cancelled"; a running one leaves before the next batched step)."""
-        _check(lib().sams_lare_serve_cancel(self._h, ticket))
+        _check(self._fn("cancel")(self._h, ticket))
 
     def release(self, ticket):
-        _check(lib().sams_lare_serve_release(self._h, ticket))
+        _check(self._fn("release")(self._h, ticket))
         self._keep.pop(ticket, None)
 
     def drain(self, timeout_s=600.0):
-        _check(lib().sams_lare_serve_drain(self._h, float(timeout_s)))
+        _check(self._fn("drain")(self._h, float(timeout_s)))
 
     def stats(self):
         s = ServeStats()
-        _check(lib().sams_lare_serve_get_stats(self._h, ctypes.byref(s)))
+        _check(self._fn("get_stats")(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServeStats._fields_}
+
+
+class Router(Server):
+    """Serving on several GPUs (include/sams_lare.h, "Serving on several
+    GPUs"): one continuous-batching server per entry of `devices` and a host
+    router that places each submitted solve on the least-loaded one.  Same
+    calls as Server; `placement(ticket)` says which server took a solve."""
+
+    _prefix = "sams_lare_router_"
+
+    def __init__(self, budget_bytes_per_device, devices=(0,), max_cells=0):
+        L = lib()
+        _bind_serve(L)
+        devs = (ctypes.c_int * len(devices))(*devices)
+        h = ctypes.c_void_p()
+        _check(L.sams_lare_router_create(devs, len(devices), int(budget_bytes_per_device), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+        self.devices = tuple(devices)
+        if max_cells:
+            self.set_max_cells(max_cells)
+
+    def placement(self, ticket):
+        idx = ctypes.c_int(-1)
+        _check(lib().sams_lare_router_placement(self._h, ticket, ctypes.byref(idx)))
+        return idx.value
+
+    def server_stats(self, index):
+        s = ServeStats()
+        _check(lib().sams_lare_router_server_stats(self._h, index, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in ServeStats._fields_}
