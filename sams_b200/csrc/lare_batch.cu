@@ -39,18 +39,24 @@ __global__ void __launch_bounds__(kT, Op::kMinBlocks)
     __shared__ Ctx c;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const Tile tl = tiles[t];
-        __syncthreads();
-        load_ctx(c, ctxs + tl.inst);
-        __syncthreads();
-        if (resistive_only && !c.p.resistive) continue;
-        const int a = arg >= 0 ? arg : c.p.resistive;
+        // threads walk the op's own (j, k) range (no idle lanes on the ghost
+        // planes of thin solves); the tiles cover the whole box plane, so
+        // every op's range is inside them, and a tile past the op's range
+        // is skipped before its context is staged (uniform over the block)
+        const Ctx *src = ctxs + tl.inst;
+        const int resistive = src->p.resistive;
+        if (resistive_only && !resistive) continue;
+        const int a = arg >= 0 ? arg : resistive;
         int lo[3], hi[3];
-        Op::bounds(c.g, a, lo, hi);
-        const int ek = c.g.nz + 5, ej = c.g.ny + 5;
+        Op::bounds(src->g, a, lo, hi);
+        const int nk = hi[2] - lo[2] + 1;
+        if (tl.p0 >= (hi[1] - lo[1] + 1) * nk || tl.i0 > hi[0] || tl.i0 + tile_i - 1 < lo[0]) continue;
+        __syncthreads();
+        load_ctx(c, src);
+        __syncthreads();
         const int p = tl.p0 + (int)threadIdx.x;
-        if (p >= ej * ek) continue;
-        const int j = -2 + p / ek, k = -2 + p % ek;
-        if (j < lo[1] || j > hi[1] || k < lo[2] || k > hi[2]) continue;
+        if (p >= (hi[1] - lo[1] + 1) * nk) continue;
+        const int j = lo[1] + p / nk, k = lo[2] + p % nk;
         const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
         for (int i = ia; i <= ib; ++i) Op::template run<GEO, P2>(c, a, i, j, k);
     }
@@ -64,23 +70,22 @@ __global__ void __launch_bounds__(kT, ops::Visc::kMinBlocks)
     __shared__ double wmin[kT / 32];
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const Tile tl = tiles[t];
+        int lo[3], hi[3];
+        ops::Visc::bounds(ctxs[tl.inst].g, 0, lo, hi);
+        const int nk = hi[2] - lo[2] + 1;
+        if (tl.p0 >= (hi[1] - lo[1] + 1) * nk || tl.i0 > hi[0] || tl.i0 + tile_i - 1 < lo[0]) continue;
         __syncthreads();
         load_ctx(c, ctxs + tl.inst);
         __syncthreads();
-        int lo[3], hi[3];
-        ops::Visc::bounds(c.g, 0, lo, hi);
-        const int ek = c.g.nz + 5, ej = c.g.ny + 5;
         const int p = tl.p0 + (int)threadIdx.x;
         double best = DBL_MAX;
         bool bad = false;
-        if (p < ej * ek) {
-            const int j = -2 + p / ek, k = -2 + p % ek;
-            if (j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
-                const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
-                for (int i = ia; i <= ib; ++i) {
-                    double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
-                    best = dev::pmin(best, cand);
-                }
+        if (p < (hi[1] - lo[1] + 1) * nk) {
+            const int j = lo[1] + p / nk, k = lo[2] + p % nk;
+            const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
+            for (int i = ia; i <= ib; ++i) {
+                double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
+                best = dev::pmin(best, cand);
             }
         }
         if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c.sc->status, 1);
