@@ -269,6 +269,32 @@ int sams_lare_router_destroy(sams_lare_router *r);
 int sams_lare_route_pick(int n, const double *pending_cell_updates, const int64_t *committed_bytes,
                          const int64_t *budget_bytes, int64_t request_bytes, int *index);
 
+/* ---- One solve on several GPUs -------------------------------------------
+ * The reference's MPI decomposition with MPIManager::haloExchange
+ * (include/harness/mpiManager.h:1246-1277), for grids larger than one GPU:
+ * the grid is cut along x into nparts slabs of nx/nparts (+1) cells, slab q
+ * on devices[q] (a device may hold several slabs).  At every boundary fill of
+ * the step each slab pulls its x ghost planes from the neighbouring slabs by
+ * peer copies; the CFL minimum is taken over all slabs.  The result equals
+ * the undivided solve's bit for bit.  Needs at least three cells per slab;
+ * rke is not available (its correction gathers over the whole grid in order). */
+typedef struct sams_lare_dist sams_lare_dist;
+
+/* Host only: offsets[0..nparts] with slab q covering cells offsets[q]+1 ..
+ * offsets[q+1] (the partition sams_lare_dist_create uses). */
+int sams_lare_dist_partition(int64_t nx, int nparts, int64_t *offsets);
+int sams_lare_dist_create(const sams_lare_params *params, const sams_lare_bcs *bcs, const int *devices, int nparts,
+                          sams_lare_dist **out);
+/* First global cell index (1-based) and cell count of slab `part`. */
+int sams_lare_dist_slab(sams_lare_dist *d, int part, int64_t *first_cell, int64_t *ncells);
+/* Whole-grid box buffers (-2..n+2 per dimension, z fastest), as for a single solve. */
+int sams_lare_dist_upload_field(sams_lare_dist *d, int field, const double *host_box);
+int sams_lare_dist_download_field(sams_lare_dist *d, int field, double *host_box);
+/* Advance nsteps timesteps on every slab; returns when they are done. */
+int sams_lare_dist_step(sams_lare_dist *d, int64_t nsteps);
+int sams_lare_dist_get_state(sams_lare_dist *d, double *dt, double *time, int64_t *step);
+int sams_lare_dist_destroy(sams_lare_dist *d);
+
 /* No counterpart in the reference.  Advance nsteps timesteps of a solve whose
  * 13 fields live in the caller's own device memory, allocating nothing: for
  * callers that cannot call cudaMalloc while running (a host code whose device

@@ -66,6 +66,24 @@ inline std::vector<double> geom_tables(const sams_lare_params &p)
     return t;
 }
 
+// The tables of an x slab (cells off+1 .. off+p.nx) of a grid of nx_global
+// cells over p.x_min..p.x_max: the whole grid's tables from row off on.
+inline std::vector<double> geom_tables_slab(const sams_lare_params &p, long long off, long long nx_global)
+{
+    sams_lare_params pg = p;
+    pg.nx = nx_global;
+    const std::vector<double> t = geom_tables(pg);
+    const size_t GX = (size_t)nx_global + 5, X = (size_t)p.nx + 5, Y = (size_t)p.ny + 5;
+    std::vector<double> s(geom_table_size(p));
+    double *o = s.data();
+    for (int a = 0; a < 4; ++a, o += X) std::copy(t.begin() + a * GX + off, t.begin() + a * GX + off + X, o);
+    const double *h2 = t.data() + 4 * GX;
+    for (int a = 0; a < 4; ++a, o += X * Y)
+        std::copy(h2 + a * GX * Y + off * Y, h2 + a * GX * Y + (off + X) * Y, o);
+    std::copy(h2 + 4 * GX * Y, h2 + 4 * GX * Y + Y, o);  // cot (per y)
+    return s;
+}
+
 // Point a GeomF at a device copy of geom_tables(p).
 inline void geom_bind(GeomF &gf, const double *dev, const sams_lare_params &p)
 {

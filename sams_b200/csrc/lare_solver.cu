@@ -256,6 +256,24 @@ static void axis_host(double lo, double hi, long long n, std::vector<double> &db
 
 int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device)
 {
+    return init_impl(p, bcs, device, nullptr);
+}
+
+int Solver::init_slab(const sams_lare_params &p, const sams_lare_bcs &bcs, int device, const XSlab &slab)
+{
+    if (slab.off < 0 || slab.off + p.nx > slab.nx_global) {
+        err = "slab outside the grid";
+        return SAMS_ERR_INVALID;
+    }
+    if (p.rke) {
+        err = "the remap kinetic-energy correction (rke) gathers over the whole grid in order; not on slabs";
+        return SAMS_ERR_UNSUPPORTED;
+    }
+    return init_impl(p, bcs, device, &slab);
+}
+
+int Solver::init_impl(const sams_lare_params &p, const sams_lare_bcs &bcs, int device, const XSlab *slab)
+{
     if (p.nx < 1 || p.ny < 1 || p.nz < 1) { err = "grid sizes must be >= 1"; return SAMS_ERR_INVALID; }
     if (p.nx > 60000 || p.ny > 60000 || p.nz > 60000) { err = "grid size too large"; return SAMS_ERR_INVALID; }
     if (p.geometry < 0 || p.geometry > 2) { err = "geometry must be 0 (Cartesian), 1 (cylindrical) or 2 (spherical)"; return SAMS_ERR_UNSUPPORTED; }
@@ -305,14 +323,21 @@ int Solver::init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device
 
     // 1-D spacings: dxb, dyb, dzb, dxc, dyc, dzc, each (n + 6) long.
     std::vector<double> dxb, dyb, dzb, dxc, dyc, dzc;
-    axis_host(p.x_min, p.x_max, p.nx, dxb, dxc);
+    if (slab) {  // the whole grid's x axis from the slab's offset on
+        std::vector<double> gb, gc;
+        axis_host(p.x_min, p.x_max, slab->nx_global, gb, gc);
+        dxb.assign(gb.begin() + slab->off, gb.begin() + slab->off + p.nx + 6);
+        dxc.assign(gc.begin() + slab->off, gc.begin() + slab->off + p.nx + 6);
+    } else {
+        axis_host(p.x_min, p.x_max, p.nx, dxb, dxc);
+    }
     axis_host(p.y_min, p.y_max, p.ny, dyb, dyc);
     axis_host(p.z_min, p.z_max, p.nz, dzb, dzc);
     std::vector<double> packed;
     for (auto *v : {&dxb, &dyb, &dzb, &dxc, &dyc, &dzc}) packed.insert(packed.end(), v->begin(), v->end());
     const size_t geo_off = packed.size();
     if (p.geometry) {  // metric factors after the spacings
-        std::vector<double> t = geom_tables(p);
+        std::vector<double> t = slab ? geom_tables_slab(p, slab->off, slab->nx_global) : geom_tables(p);
         packed.insert(packed.end(), t.begin(), t.end());
     }
     if ((rc = check(cudaMalloc(&axes_, packed.size() * sizeof(double)), "cudaMalloc(axes)"))) return rc;
@@ -493,6 +518,12 @@ void Solver::bc_fill(unsigned mask)
 {
     FieldList fl = make_list(mask);
     if (fl.n == 0) return;
+    if (halo_) {  // a slab: x by exchange, then y and z in the same order as below
+        halo_->fill_x(*this, mask);
+        bc_fill_dim(mask, 1);
+        bc_fill_dim(mask, 2);
+        return;
+    }
     const Geom &g = ctx_.g;
     // the one-pass gather needs every source inside the domain (n >= 3)
     if (all_periodic(mask) && std::min(g.nx, std::min(g.ny, g.nz)) >= kBcSequentialBelow) {
@@ -510,6 +541,15 @@ void Solver::bc_fill(unsigned mask)
 
 void Solver::bc_fill_dim(unsigned mask, int d)
 {
+    if (halo_ && d == 0) {
+        halo_->fill_x(*this, mask);
+        return;
+    }
+    for (int e = 0; e < 2; ++e) bc_fill_edge(mask, d, e);
+}
+
+void Solver::bc_fill_edge(unsigned mask, int d, int e)
+{
     FieldList fl = make_list(mask);
     if (fl.n == 0) return;
     const Geom &g = ctx_.g;
@@ -518,10 +558,8 @@ void Solver::bc_fill_dim(unsigned mask, int d)
     for (int q = 0; q < 3; ++q)
         if (q != d) slab *= ext[q];
     dim3 grid((unsigned)ceil_div(slab, kThreads), (unsigned)fl.n);
-    for (int e = 0; e < 2; ++e) {
-        k_bc_edge<<<grid, kThreads, 0, stream_>>>(ctx_, fl, bc_, d, e);
-        ++launches_;
-    }
+    k_bc_edge<<<grid, kThreads, 0, stream_>>>(ctx_, fl, bc_, d, e);
+    ++launches_;
 }
 
 void Solver::enqueue_step(cudaEvent_t *marks)
@@ -549,6 +587,7 @@ void Solver::enqueue_step(cudaEvent_t *marks)
             k_visc<false, false><<<grid, kThreads, 0, stream_>>>(ctx_);
         ++launches_;
     }
+    if (halo_) halo_->reduce_dt(*this);
     k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);
     ++launches_;
     if (resistive) {

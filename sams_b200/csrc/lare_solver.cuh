@@ -30,6 +30,27 @@ enum : unsigned {
     FM_ALL9 = FM_BFIELD | FM_ENERGY | FM_DENSITY | FM_VELOCITY
 };
 
+class Solver;
+
+// A solve split along x into slabs (lare_dist.cu): the slab's place in the
+// whole grid, and the hooks that replace the x boundary fills (halo
+// exchange with the neighbouring slabs) and complete the CFL minimum over
+// all slabs.
+struct XSlab {
+    long long off = 0;        // global index of the slab's cell 0 (cells off+1 .. off+nx)
+    long long nx_global = 0;  // cells of the whole grid along x
+};
+
+class Halo {
+public:
+    virtual ~Halo() = default;
+    // Fill the x ghost planes of the fields in mask (exchange at slab
+    // edges, the boundary condition at the grid's own edges).
+    virtual void fill_x(Solver &s, unsigned mask) = 0;
+    // Replace this slab's CFL candidate minimum by the minimum over all slabs.
+    virtual void reduce_dt(Solver &s) = 0;
+};
+
 class Solver {
 public:
     Solver() = default;
@@ -39,6 +60,17 @@ public:
 
     // Returns a sams_status; on failure err holds the reason.
     int init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device);
+    // One x slab of a larger grid: p.nx is the slab's own cell count, the
+    // x axis and metric tables are those of the whole grid (slab.nx_global
+    // cells over x_min..x_max) from the slab's offset on.
+    int init_slab(const sams_lare_params &p, const sams_lare_bcs &bcs, int device, const XSlab &slab);
+    void set_halo(Halo *h) { halo_ = h; }
+    cudaStream_t stream() const { return stream_; }
+    Scalars *scalars_ptr() const { return sc_; }
+    int device() const { return device_; }
+    const BcTable &bc_table() const { return bc_; }
+    // Boundary-condition fill of one (dimension, edge) for the fields in mask.
+    void bc_fill_edge(unsigned mask, int dim, int edge);
     // Set up over memory the solver does not own (fields, scratch, axes and
     // scalars already placed in ctx); allocates nothing and frees nothing.
     int init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, const Ctx &ctx, int device,
@@ -78,8 +110,11 @@ private:
     int staging(double **out);
     void free_all();
 
+    int init_impl(const sams_lare_params &p, const sams_lare_bcs &bcs, int device, const XSlab *slab);
+
     sams_lare_params p_{};
     BcTable bc_{};
+    Halo *halo_ = nullptr;
     int device_ = 0;
     int sm_count_ = 148;  // multiprocessors of device_ (grid sizing)
     cudaStream_t own_stream_ = nullptr;

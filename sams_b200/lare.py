@@ -531,3 +531,91 @@ class Router(Server):
         s = ServeStats()
         _check(lib().sams_lare_router_server_stats(self._h, index, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in ServeStats._fields_}
+
+
+def _bind_dist(L):
+    if getattr(L, "_dist_bound", False):
+        return
+    vp, i64 = ctypes.c_void_p, ctypes.c_int64
+    L.sams_lare_dist_partition.argtypes = [i64, ctypes.c_int, ctypes.POINTER(i64)]
+    L.sams_lare_dist_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(Bcs), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.c_int, ctypes.POINTER(vp)]
+    L.sams_lare_dist_slab.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    L.sams_lare_dist_upload_field.argtypes = [vp, ctypes.c_int, _P]
+    L.sams_lare_dist_download_field.argtypes = [vp, ctypes.c_int, _P]
+    L.sams_lare_dist_step.argtypes = [vp, i64]
+    L.sams_lare_dist_get_state.argtypes = [vp, _P, _P, ctypes.POINTER(i64)]
+    L.sams_lare_dist_destroy.argtypes = [vp]
+    L._dist_bound = True
+
+
+def dist_partition(nx, nparts):
+    """Cell offsets of the x slabs of a distributed solve: slab q covers
+    cells offsets[q]+1 .. offsets[q+1] (host only)."""
+    L = lib()
+    _bind_dist(L)
+    out = (ctypes.c_int64 * (nparts + 1))()
+    _check(L.sams_lare_dist_partition(int(nx), int(nparts), out))
+    return list(out)
+
+
+class DistLARE3D:
+    """One LARE3D solve cut along x into slabs over several GPUs (the
+    reference's MPI decomposition, include/harness/mpiManager.h:1246-1277):
+    slab q runs on devices[q]; ghost planes move between slabs by peer
+    copies at every boundary fill.  Whole-grid box arrays in and out, as for
+    LARE3D."""
+
+    name = "LARE3D"
+
+    def __init__(self, params, bcs, devices):
+        L = lib()
+        _bind_dist(L)
+        self.params = params
+        self.shape = box_shape(params.nx, params.ny, params.nz)
+        devs = (ctypes.c_int * len(devices))(*devices)
+        h = ctypes.c_void_p()
+        _check(L.sams_lare_dist_create(ctypes.byref(params), ctypes.byref(bcs), devs, len(devices),
+                                       ctypes.byref(h)))
+        self._h = h
+        self.devices = tuple(devices)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sams_lare_dist_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def slab(self, part):
+        first, n = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().sams_lare_dist_slab(self._h, part, ctypes.byref(first), ctypes.byref(n)))
+        return first.value, n.value
+
+    def upload(self, field, arr):
+        idx = FIELD[field] if isinstance(field, str) else field
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.shape == self.shape
+        _check(lib().sams_lare_dist_upload_field(self._h, idx, a.ctypes.data_as(_P)))
+
+    def upload_all(self, fields):
+        for f, a in enumerate(fields):
+            self.upload(f, a)
+
+    def download(self, field, out=None):
+        idx = FIELD[field] if isinstance(field, str) else field
+        out = np.empty(self.shape) if out is None else out
+        _check(lib().sams_lare_dist_download_field(self._h, idx, out.ctypes.data_as(_P)))
+        return out
+
+    def step(self, n=1):
+        _check(lib().sams_lare_dist_step(self._h, int(n)))
+
+    def state(self):
+        dt, tm, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _check(lib().sams_lare_dist_get_state(self._h, ctypes.byref(dt), ctypes.byref(tm), ctypes.byref(st)))
+        return dt.value, tm.value, st.value
