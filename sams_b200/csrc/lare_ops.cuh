@@ -1260,5 +1260,37 @@ struct RkeEnergy {
 
 #undef LOFF
 
+// Register cap (blocks of 256 per SM) of an op's power-of-two instantiation:
+// multiplying by reciprocals instead of calling the division routine lets
+// the compiler keep more values live, so these caps were tuned separately
+// on B200 (the same sweep as kMinBlocks, on the 256^3 step).
+template <class Op>
+struct CapP2 {
+    static constexpr int value = Op::kMinBlocks;
+};
+template <>
+struct CapP2<Visc> {
+    static constexpr int value = 2;
+};
+template <>
+struct CapP2<NodePrep> {
+    static constexpr int value = 5;
+};
+template <>
+struct CapP2<ResistRK> {
+    static constexpr int value = 5;
+};
+template <>
+struct CapP2<Pred1> {
+    static constexpr int value = 6;
+};
+
 }  // namespace ops
+
+// Blocks-per-SM bound of a kernel running Op.
+template <class Op, bool P2>
+struct MinBlocks {
+    static constexpr int value = P2 ? ops::CapP2<Op>::value : Op::kMinBlocks;
+};
+
 }  // namespace sams

@@ -32,7 +32,7 @@ constexpr int kThreads = 256;
 // geometry is curvilinear (its metric factors are applied); the Cartesian
 // instantiation has no trace of them.
 template <class Op, bool GEO, bool P2>
-__global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
+__global__ void __launch_bounds__(kThreads, (MinBlocks<Op, P2>::value)) k_op(Ctx c, int arg)
 {
     int lo[3], hi[3];
     Op::bounds(c.g, arg, lo, hi);
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kThreads, Op::kMinBlocks) k_op(Ctx c, int arg)
 // them into Scalars::dtmin_bits.  Positive doubles order like their bit
 // patterns, so an integer atomicMin is an exact, order-free minimum.
 template <bool GEO, bool P2>
-__global__ void __launch_bounds__(kThreads, ops::Visc::kMinBlocks) k_visc(Ctx c)
+__global__ void __launch_bounds__(kThreads, (MinBlocks<ops::Visc, P2>::value)) k_visc(Ctx c)
 {
     int lo[3], hi[3];
     ops::Visc::bounds(c.g, 0, lo, hi);
