@@ -32,7 +32,7 @@ __device__ __forceinline__ void load_ctx(Ctx &dst, const Ctx *src)
 // GEO: some solve of the batch is curvilinear (the Cartesian instantiation,
 // used when none is, carries no metric factors).
 template <class Op, bool GEO, bool P2>
-__global__ void __launch_bounds__(kT, (MinBlocks<Op, P2>::value))
+__global__ void __launch_bounds__(kT, (MinBlocksBatch<Op, P2>::value))
     kb_op(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int arg, int tile_i,
           int resistive_only)
 {
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kT, (MinBlocks<Op, P2>::value))
 }
 
 template <bool GEO, bool P2>
-__global__ void __launch_bounds__(kT, (MinBlocks<ops::Visc, P2>::value))
+__global__ void __launch_bounds__(kT, (MinBlocksBatch<ops::Visc, P2>::value))
     kb_visc(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int tile_i)
 {
     __shared__ Ctx c;

@@ -1285,12 +1285,34 @@ struct CapP2<Pred1> {
     static constexpr int value = 6;
 };
 
+// Register cap of an op in the batched engine (lare_batch.cu), whose solves
+// are typically thin (n x n x 4): rows of nine doubles, tiles of eight
+// planes.  Swept on B200 like kMinBlocks, on the batched step of 64
+// Orszag-Tang solves; ops not listed keep kMinBlocks.
+template <class Op>
+struct CapBatch {
+    static constexpr int value = Op::kMinBlocks;
+};
+template <> struct CapBatch<Visc> { static constexpr int value = 4; };
+template <> struct CapBatch<BScale> { static constexpr int value = 8; };
+template <> struct CapBatch<SweepCvc> { static constexpr int value = 8; };
+template <> struct CapBatch<Corr2> { static constexpr int value = 5; };
+template <int D> struct CapBatch<SweepVol<D>> { static constexpr int value = 4; };
+template <int D> struct CapBatch<SweepCTUpd<D>> { static constexpr int value = 8; };
+template <int D> struct CapBatch<SweepMass<D>> { static constexpr int value = 4; };
+template <int D> struct CapBatch<SweepS7<D>> { static constexpr int value = 4; };
+template <int D> struct CapBatch<SweepS8<D>> { static constexpr int value = 8; };
+
 }  // namespace ops
 
 // Blocks-per-SM bound of a kernel running Op.
 template <class Op, bool P2>
 struct MinBlocks {
     static constexpr int value = P2 ? ops::CapP2<Op>::value : Op::kMinBlocks;
+};
+template <class Op, bool P2>
+struct MinBlocksBatch {
+    static constexpr int value = P2 ? ops::CapP2<Op>::value : ops::CapBatch<Op>::value;
 };
 
 }  // namespace sams
