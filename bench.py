@@ -36,8 +36,17 @@ UNIT = "cell-updates/s"
 # per phase, 8 B per value (dt pass 72, predictor 96, corrector 144, three
 # sweeps 3 x 176, two resistive sub-steps 2 x 72).
 ALGO_BYTES_PER_CELL_UPDATE = 984
-WORKLOAD = ("plain LARE3D step, 256^3 periodic random-field cube [0,1]^3, rho=1, p=0.1, "
+def workload(n):
+    return (f"plain LARE3D step, {n}^3 periodic random-field cube [0,1]^3, rho=1, p=0.1, "
             "|B|rms=0.1, |v|rms=0.05, k=1..8, gamma=5/3, eta=1e-4 (resistive), seeded synthetic IC")
+
+
+def l2_note(n):
+    """How the timed inputs relate to the 126 MB L2 of a B200."""
+    field_mb = (n + 5) * (n + 5) * (((n + 6) + 7) // 8 * 8) * 8 / 1e6
+    if field_mb * 32 > 126:
+        return f"inputs larger than L2 (each field {field_mb:.0f} MB, 32 x {field_mb:.0f} MB resident)"
+    return f"inputs fit in L2 (each field {field_mb:.1f} MB): not a full-size run"
 
 
 def parse():
@@ -203,7 +212,7 @@ def run_reference_arm(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "case": "rf", "grid": [n, n, n], "parallelism": "cpu-openmp"},
+        "config": {"workload": workload(n), "case": "rf", "grid": [n, n, n], "parallelism": "cpu-openmp"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{len(timed)} timed steps of the {n}^3 workload after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -321,9 +330,9 @@ def run_sams(args, world, rank, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "case": "rf", "grid": [n, n, n],
+        "config": {"workload": workload(n), "case": "rf", "grid": [n, n, n],
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (each field 144 MB, 32 x 144 MB resident)"},
+                   "l2": l2_note(n)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": launches * args.steps,
         "batched": batched,
