@@ -392,7 +392,7 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     c.gf = GeomF{};
     if (p.geometry) geom_bind(c.gf, s.axes + geo_off, p);
     c.p.geometry = (int)p.geometry;
-    c.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, &c.rc) ? 1 : 0;
+    c.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, p.mu0, &c.rc) ? 1 : 0;
     c.p.gamma = p.gas_gamma;
     c.p.mu0 = p.mu0;
     c.p.visc1 = p.visc1;

@@ -65,6 +65,7 @@ struct Phys {
 // every operand, so kernels built for such grids multiply instead.
 struct Recip {
     double xb, yb, zb, xc, yc, zc, cv;
+    double mu0;  // 1 / mu0 (mu0 is a power of two too)
 };
 
 // Metric factors of a cylindrical or spherical solve, as LARE3D::grid builds

@@ -100,11 +100,12 @@ inline void geom_bind(GeomF &gf, const double *dev, const sams_lare_params &p)
 }
 
 // True when every spacing array (as the axis builders lay them out: index
-// i + 2, b over -2..n+2, c over -1..n+2) holds one value per axis and that
-// value is a power of two; fills the reciprocals (exact for powers of two).
+// i + 2, b over -2..n+2, c over -1..n+2) holds one value per axis, that
+// value is a power of two, and so is mu0; fills the reciprocals (exact for
+// powers of two).
 inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> &dyb, const std::vector<double> &dzb,
                       const std::vector<double> &dxc, const std::vector<double> &dyc, const std::vector<double> &dzc,
-                      Recip *rc)
+                      double mu0, Recip *rc)
 {
     auto uniform = [](const std::vector<double> &d, size_t from, size_t to, double *v) {
         if (d.size() < to || from >= to) return false;
@@ -117,6 +118,8 @@ inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> 
         return true;
     };
     double xb, yb, zb, xc, yc, zc;
+    int e;
+    if (!(mu0 > 0.0) || !(mu0 < DBL_MAX) || std::frexp(mu0, &e) != 0.5) return false;
     // b: array indices 0 .. n+4 (i = -2 .. n+2); c: 1 .. n+4 (i = -1 .. n+2)
     if (!uniform(dxb, 0, dxb.size() - 1, &xb) || !uniform(dyb, 0, dyb.size() - 1, &yb) ||
         !uniform(dzb, 0, dzb.size() - 1, &zb) || !uniform(dxc, 1, dxc.size() - 1, &xc) ||
@@ -129,6 +132,7 @@ inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> 
     rc->yc = 1.0 / yc;
     rc->zc = 1.0 / zc;
     rc->cv = 1.0 / (xb * (yb * zb));
+    rc->mu0 = 1.0 / mu0;
     return true;
 }
 

@@ -305,7 +305,7 @@ struct Visc {
                           (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double rho0 = pmax(rho, NONE_ZERO);
         double cs2 = gm * pressure / rho0;
-        double w1 = (bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o]) / c.p.mu0 / rho0;
+        double w1 = div_by<P2>(bx[o] * bx[o] + by[o] * by[o] + bz[o] * bz[o], c.p.mu0, c.rc.mu0) / rho0;
         double c_visc2 = p_visc / rho0;
         // outside Cartesian geometry the CFL range starts at x index 1 (lagran.cpp:384)
         if (GEO && c.p.geometry && i < 1) return DBL_MAX;
@@ -607,9 +607,9 @@ struct Pred2 {
         double bzv = SUM8(bz1) / (cvx + cvxp);
 #undef SUM8
         const double mu0 = c.p.mu0;
-        fx += (jy * bzv - jz * byv) / mu0;
-        fy += (jz * bxv - jx * bzv) / mu0;
-        fz += (jx * byv - jy * bxv) / mu0;
+        fx += div_by<P2>(jy * bzv - jz * byv, mu0, c.rc.mu0);
+        fy += div_by<P2>(jz * bxv - jx * bzv, mu0, c.rc.mu0);
+        fz += div_by<P2>(jx * byv - jy * bxv, mu0, c.rc.mu0);
         if (geo) {  // geometric source terms (lagran.cpp:711-721)
             const double rv = __ldg(c.s[S_RHOV] + o), r = c.gf.xb[i + 2];
             const double ux = __ldg(c.f[SAMS_F_VX] + o), uy = __ldg(c.f[SAMS_F_VY] + o), uz = __ldg(c.f[SAMS_F_VZ] + o);

@@ -352,7 +352,7 @@ int Solver::init_impl(const sams_lare_params &p, const sams_lare_bcs &bcs, int d
     ctx_.gf = GeomF{};
     if (p.geometry) geom_bind(ctx_.gf, axes_ + geo_off, p);
     ctx_.p.geometry = (int)p.geometry;
-    ctx_.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, &ctx_.rc) ? 1 : 0;
+    ctx_.p.pow2 = p.geometry == 0 && pow2_grid(dxb, dyb, dzb, dxc, dyc, dzc, p.mu0, &ctx_.rc) ? 1 : 0;
 
     ctx_.p.gamma = p.gas_gamma;
     ctx_.p.mu0 = p.mu0;
