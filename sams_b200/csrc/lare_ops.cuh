@@ -1134,6 +1134,103 @@ struct SweepS8 {
     }
 };
 
+// The z sweep's SweepS6, SweepS7 and SweepS8 as three stages of one kernel
+// (k_zsweep) over whole z lines.  Every value one stage passes to the next
+// is read only along z, on the same (i, j) line, so a block that holds whole
+// lines keeps them in shared memory: the energy fluxes, node cv2, vertex
+// density, node dm and shifted v1 of stage A and the momentum fluxes of
+// stage B never go to global memory.  Each stage is the same arithmetic as
+// the separate kernel it replaces.  Shared arrays are indexed by k + 2 from
+// the line's base (k = -2 .. nz+1); the kernel separates the stages with
+// __syncthreads.  Not used with rke (its correction needs the raw fluxes).
+struct SweepZ678 {
+    enum { FE1, FE2, CV2N, RVN, DMN, V1S, FM1, FM2, FM3, NARR };
+
+    // SweepS6<2> at (i, j, k), k = -2..nz+1; returns the new rho (or 0).
+    template <bool GEO>
+    __device__ static double stage_a(const Ctx &c, int i, int j, int k, double *sm, int at, int S)
+    {
+        const Geom &g = c.g;
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const double dt = c.sc->dt;
+        const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
+        const RO dm{c.f[SAMS_F_DM]};
+        double rho_new = 0.0;
+        if (i >= 1 && j >= 1 && k >= 1 && k <= g.nz) {
+            rho_new = (rho1[o] * cv1[o] + dm[o - 1] - dm[o]) / cv2[o];
+            c.f[SAMS_F_RHO][o] = rho_new;
+        }
+        if (k >= 0 && k <= g.nz) {
+            double v = face_velocity<2>(c, o);
+            double area = face_area<2, GEO>(c, i, j, k);
+            const RO ee{c.f[SAMS_F_ENERGY_ELECTRON]}, ei{c.f[SAMS_F_ENERGY_ION]};
+            sm[FE1 * S + at] = energy_flux(v, dt, area, ee[o - 1], ee[o], ee[o + 1], ee[o + 2], cvc1[o], cvc1[o - 1],
+                                           cvc1[o + 1], cv1[o], cv1[o + 1], rho1[o], rho1[o + 1], dm[o]);
+            sm[FE2 * S + at] = energy_flux(v, dt, area, ei[o - 1], ei[o], ei[o + 1], ei[o + 2], cvc1[o], cvc1[o - 1],
+                                           cvc1[o + 1], cv1[o], cv1[o + 1], rho1[o], rho1[o + 1], dm[o]);
+            sm[CV2N * S + at] = (cv2[o] + cv2[o + SX] + cv2[o + SY] + cv2[o + SX + SY] + cv2[o + 1] + cv2[o + SX + 1] +
+                                 cv2[o + SY + 1] + cv2[o + SX + SY + 1]) * 0.125;
+        }
+        if (k >= -1) {
+            double sum = rho1[o] * cv1[o] + rho1[o + SX] * cv1[o + SX] + rho1[o + SY] * cv1[o + SY] +
+                         rho1[o + SX + SY] * cv1[o + SX + SY] + rho1[o + 1] * cv1[o + 1] +
+                         rho1[o + SX + 1] * cv1[o + SX + 1] + rho1[o + SY + 1] * cv1[o + SY + 1] +
+                         rho1[o + SX + SY + 1] * cv1[o + SX + SY + 1];
+            sm[RVN * S + at] = sum * (0.125 / cvc1[o]);
+        }
+        if (k >= -1 && k <= g.nz)
+            sm[DMN * S + at] = (dm[o] + dm[o + SX] + dm[o + SY] + dm[o + SX + SY] + dm[o + 1] + dm[o + SX + 1] +
+                                dm[o + SY + 1] + dm[o + SX + SY + 1]) * 0.125;
+        const RO v1{c.f[SAMS_F_VZ1]};
+        sm[V1S * S + at] = (v1[o] + v1[o + 1]) * 0.5;
+        return rho_new;
+    }
+
+    // SweepS7<2> at (i, j, k), k = -1..nz.
+    template <bool GEO>
+    __device__ static void stage_b(const Ctx &c, int i, int j, int k, double *sm, int at, int S, double rho_new)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        const double dt = c.sc->dt;
+        const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
+        if (i >= 1 && j >= 1 && k >= 1) {
+            double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+            double den = cv2[o] * rho_new;
+            ee[o] = (ee[o] * cv1[o] * rho1[o] + sm[FE1 * S + at - 1] - sm[FE1 * S + at]) / den;
+            ei[o] = (ei[o] * cv1[o] * rho1[o] + sm[FE2 * S + at - 1] - sm[FE2 * S + at]) / den;
+        }
+        double area = dyac_at<GEO>(c, i, j, k);  // the z sweep uses dyac (zremap.cpp:475)
+        const double v = sm[V1S * S + at], dmv = sm[DMN * S + at];
+        const double dci = cv1[o + 1], dcm = cv1[o], dcp = cv1[o + 2], cvi = cvc1[o], cvp = cvc1[o + 1];
+        const double rvi = sm[RVN * S + at], rvp = sm[RVN * S + at + 1];
+        const RO ux{c.f[SAMS_F_VX]}, uy{c.f[SAMS_F_VY]}, uz{c.f[SAMS_F_VZ]};
+        const double f1 = mom_flux<true>(v, dt, area, ux[o - 1], ux[o], ux[o + 1], ux[o + 2], dci, dcm, dcp, cvi, cvp,
+                                         rvi, rvp, dmv);
+        const double f2 = mom_flux<true>(v, dt, area, uy[o - 1], uy[o], uy[o + 1], uy[o + 2], dci, dcm, dcp, cvi, cvp,
+                                         rvi, rvp, dmv);
+        const double f3 = mom_flux<true>(v, dt, area, uz[o - 1], uz[o], uz[o + 1], uz[o + 2], dci, dcm, dcp, cvi, cvp,
+                                         rvi, rvp, dmv);
+        sm[FM1 * S + at] = f1 * dmv;
+        sm[FM2 * S + at] = f2 * dmv;
+        sm[FM3 * S + at] = f3 * dmv;
+    }
+
+    // SweepS8<2> at (i, j, k), k = 0..nz.
+    __device__ static void stage_c(const Ctx &c, int i, int j, int k, const double *sm, int at, int S)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        const double rvo = sm[RVN * S + at], cvco = __ldg(c.s[S_R_CVC1] + o), cv2o = sm[CV2N * S + at];
+        const double rho_v1 = (rvo * cvco + sm[DMN * S + at - 1] - sm[DMN * S + at]) / cv2o;
+        const double den = cv2o * rho_v1;
+        double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
+        ux[o] = (rvo * ux[o] * cvco + sm[FM1 * S + at - 1] - sm[FM1 * S + at]) / den;
+        uy[o] = (rvo * uy[o] * cvco + sm[FM2 * S + at - 1] - sm[FM2 * S + at]) / den;
+        uz[o] = (rvo * uz[o] * cvco + sm[FM3 * S + at - 1] - sm[FM3 * S + at]) / den;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Remap kinetic-energy correction (rke; Phys::rke, Ctx::dke)
 // ---------------------------------------------------------------------------

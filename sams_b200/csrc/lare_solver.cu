@@ -45,6 +45,30 @@ __global__ void __launch_bounds__(kThreads, (MinBlocks<Op, P2>::value)) k_op(Ctx
     for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::template run<GEO, P2>(c, arg, i, j, k);
 }
 
+// The z sweep's stages S6, S7 and S8 (ops::SweepZ678) over whole z lines:
+// a block holds kZThreads / (nz + 4) lines of (i, j) in 0..nx x 0..ny, one
+// thread per k = -2..nz+1 of each.
+constexpr int kZThreads = 288;
+
+template <bool GEO>
+__global__ void __launch_bounds__(kZThreads, 3) k_zsweep(Ctx c)
+{
+    extern __shared__ double zsm[];
+    const Geom &g = c.g;
+    const int W = g.nz + 4, lines = kZThreads / W, S = lines * W;
+    const int line = (int)threadIdx.x / W, k = (int)threadIdx.x % W - 2;
+    const long long q = (long long)blockIdx.x * lines + line;
+    const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
+    const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
+    const int at = line * W + k + 2;
+    double rho_new = 0.0;
+    if (on) rho_new = ops::SweepZ678::stage_a<GEO>(c, i, j, k, zsm, at, S);
+    __syncthreads();
+    if (on && k >= -1 && k <= g.nz) ops::SweepZ678::stage_b<GEO>(c, i, j, k, zsm, at, S, rho_new);
+    __syncthreads();
+    if (on && k >= 0 && k <= g.nz) ops::SweepZ678::stage_c(c, i, j, k, zsm, at, S);
+}
+
 // Visc with the CFL minimum: each block reduces its candidates and folds
 // them into Scalars::dtmin_bits.  Positive doubles order like their bit
 // patterns, so an integer atomicMin is an exact, order-free minimum.
@@ -645,13 +669,26 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     launch<ops::SweepCTUpd<2>>(0);
     launch<ops::SweepMass<2>>(0);
     bc_fill_dim(FM_DM, 2);
-    launch<ops::SweepS6<2>>(0);
-    launch<ops::SweepS7<2>>(0);
-    if (p_.rke) {
-        launch<ops::SweepRkeDk<2>>(0);
-        launch<ops::SweepRkeGather<2>>(0);
+    if (!p_.rke && ctx_.g.nz + 4 <= kZThreads) {
+        const Geom &g = ctx_.g;
+        const int W = g.nz + 4, lines = kZThreads / W;
+        const long long nl = (long long)(g.nx + 1) * (g.ny + 1);
+        const size_t smem = (size_t)ops::SweepZ678::NARR * lines * W * sizeof(double);
+        const unsigned blocks = (unsigned)ceil_div(nl, lines);
+        if (ctx_.p.geometry)
+            k_zsweep<true><<<blocks, kZThreads, smem, stream_>>>(ctx_);
+        else
+            k_zsweep<false><<<blocks, kZThreads, smem, stream_>>>(ctx_);
+        ++launches_;
+    } else {
+        launch<ops::SweepS6<2>>(0);
+        launch<ops::SweepS7<2>>(0);
+        if (p_.rke) {
+            launch<ops::SweepRkeDk<2>>(0);
+            launch<ops::SweepRkeGather<2>>(0);
+        }
+        launch<ops::SweepS8<2>>(0);
     }
-    launch<ops::SweepS8<2>>(0);
     bc_fill(FM_ALL9);
     launch<ops::BScale>(1);
     bc_fill(FM_BFIELD);
