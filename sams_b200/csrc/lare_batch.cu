@@ -100,6 +100,38 @@ __global__ void __launch_bounds__(kT, (MinBlocksBatch<ops::Visc, P2>::value))
     }
 }
 
+// The z sweep's S6, S7 and S8 as one kernel over whole z lines (the
+// single-solve k_zsweep): each tile is a run of lines of one solve,
+// kThreads / (nz + 4) of them, starting at line p0 of (i, j) in
+// 0..nx x 0..ny.
+template <bool GEO>
+__global__ void __launch_bounds__(ops::SweepZ678::kThreads, 4)
+    kb_zsweep(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles)
+{
+    __shared__ Ctx c;
+    extern __shared__ double zsm[];
+    constexpr int kZT = ops::SweepZ678::kThreads;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const Tile tl = tiles[t];
+        __syncthreads();
+        load_ctx(c, ctxs + tl.inst);
+        __syncthreads();
+        const Geom &g = c.g;
+        const int W = g.nz + 4, lines = kZT / W, S = lines * W;
+        const int line = (int)threadIdx.x / W, k = (int)threadIdx.x % W - 2;
+        const long long q = (long long)tl.p0 + line;
+        const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
+        const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
+        const int at = line * W + k + 2;
+        double rho_new = 0.0;
+        if (on) rho_new = ops::SweepZ678::stage_a<GEO>(c, i, j, k, zsm, at, S);
+        __syncthreads();
+        if (on && k >= -1 && k <= g.nz) ops::SweepZ678::stage_b<GEO>(c, i, j, k, zsm, at, S, rho_new);
+        __syncthreads();
+        if (on && k >= 0 && k <= g.nz) ops::SweepZ678::stage_c(c, i, j, k, zsm, at, S);
+    }
+}
+
 // Per-solve CFL finalisation (the single-solve k_dt_finalize, one thread per
 // live solve).
 __global__ void kb_dt_finalize(const Ctx *__restrict__ ctxs, const int *__restrict__ live, int nlive)
@@ -506,11 +538,25 @@ int Batch::rebuild()
     }
     nlive_ = (int)live.size();
     ntiles_ = (int)tiles.size();
+    // z-line tiles of the fused z sweep, after the plane tiles; used when no
+    // solve needs the raw momentum fluxes (rke) and every z line fits a block
+    constexpr int kZT = ops::SweepZ678::kThreads;
+    zfuse_ = nlive_ > 0 && !has_rke_;
+    for (int q : live)
+        if (slots_[q].ctx.g.nz + 4 > kZT) zfuse_ = false;
+    if (zfuse_)
+        for (int q : live) {
+            const Geom &g = slots_[q].ctx.g;
+            const int lpb = kZT / (g.nz + 4);
+            const long long nl = (long long)(g.nx + 1) * (g.ny + 1);
+            for (long long first = 0; first < nl; first += lpb) tiles.push_back(Tile{q, 0, (int)first, 0});
+        }
+    nztiles_ = (int)tiles.size() - ntiles_;
     shell_total_ = shell;
     for (int d = 0; d < 3; ++d) slab_total_[d] = slab[d];
     // one device buffer for all tables
     const size_t nslot = slots_.size() ? slots_.size() : 1;
-    const size_t need = nslot * sizeof(Ctx) + nslot * sizeof(BcTable) + (size_t)std::max(ntiles_, 1) * sizeof(Tile) +
+    const size_t need = nslot * sizeof(Ctx) + nslot * sizeof(BcTable) + std::max<size_t>(tiles.size(), 1) * sizeof(Tile) +
                         (size_t)std::max(nlive_, 1) * (sizeof(int) + sizeof(unsigned) + 4 * sizeof(long long)) + 1024;
     int rc;
     if (need > table_cap_bytes_) {
@@ -527,7 +573,7 @@ int Batch::rebuild()
     o += nslot * sizeof(BcTable);
     o = (o + 15) / 16 * 16;
     d_tiles_ = reinterpret_cast<Tile *>(base + o);
-    o += (size_t)std::max(ntiles_, 1) * sizeof(Tile);
+    o += std::max<size_t>(tiles.size(), 1) * sizeof(Tile);
     o = (o + 15) / 16 * 16;
     d_live_ = reinterpret_cast<int *>(base + o);
     o += (size_t)std::max(nlive_, 1) * sizeof(int);
@@ -571,6 +617,18 @@ void Batch::launch(int arg, bool resistive_only)
         kb_op<Op, false, true><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, ro);
     else
         kb_op<Op, false, false><<<grid, kT, 0, stream_>>>(d_ctx_, d_tiles_, ntiles_, arg, tile_i_, ro);
+}
+
+void Batch::launch_zsweep()
+{
+    if (nztiles_ == 0) return;
+    constexpr int kZT = ops::SweepZ678::kThreads;
+    const int grid = std::min(nztiles_, sm_count_ * 4);
+    const size_t smem = (size_t)ops::SweepZ678::NARR * kZT * sizeof(double);
+    if (has_geo_)
+        kb_zsweep<true><<<grid, kZT, smem, stream_>>>(d_ctx_, d_tiles_ + ntiles_, nztiles_);
+    else
+        kb_zsweep<false><<<grid, kZT, smem, stream_>>>(d_ctx_, d_tiles_ + ntiles_, nztiles_);
 }
 
 void Batch::launch_visc()
@@ -675,13 +733,17 @@ void Batch::enqueue_step()
     launch<ops::SweepCTUpd<2>>(0, false);
     launch<ops::SweepMass<2>>(0, false);
     bc_fill_dim(FM_DM, 2, false);
-    launch<ops::SweepS6<2>>(0, false);
-    launch<ops::SweepS7<2>>(0, false);
-    if (has_rke_) {  // solves without rke return at once (Phys::rke)
-        launch<ops::SweepRkeDk<2>>(0, false);
-        launch<ops::SweepRkeGather<2>>(0, false);
+    if (zfuse_) {
+        launch_zsweep();
+    } else {
+        launch<ops::SweepS6<2>>(0, false);
+        launch<ops::SweepS7<2>>(0, false);
+        if (has_rke_) {  // solves without rke return at once (Phys::rke)
+            launch<ops::SweepRkeDk<2>>(0, false);
+            launch<ops::SweepRkeGather<2>>(0, false);
+        }
+        launch<ops::SweepS8<2>>(0, false);
     }
-    launch<ops::SweepS8<2>>(0, false);
     bc_fill(FM_ALL9, false);
     launch<ops::BScale>(1, false);
     bc_fill(FM_BFIELD, false);

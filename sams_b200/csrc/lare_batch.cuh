@@ -74,6 +74,7 @@ private:
     void enqueue_step();
     template <class Op> void launch(int arg, bool resistive_only);
     void launch_visc();
+    void launch_zsweep();
     void bc_fill(unsigned mask, bool resistive_only);
     void bc_fill_dim(unsigned mask, int dim, bool resistive_only);
     void drop_graphs();
@@ -89,8 +90,10 @@ private:
     int sm_count_ = 148;
     // device tables (rebuilt when the set of solves changes)
     Ctx *d_ctx_ = nullptr;
-    Tile *d_tiles_ = nullptr;
+    Tile *d_tiles_ = nullptr;  // plane tiles, then (when zfuse_) the z-line tiles
     int ntiles_ = 0;
+    int nztiles_ = 0;
+    bool zfuse_ = false;  // the z sweep's S6-S8 run as one kernel (kb_zsweep)
     int *d_live_ = nullptr;
     unsigned *d_pf_ = nullptr;          // per live solve: fields that are all-periodic
     BcTable *d_bc_ = nullptr;           // per slot boundary conditions

@@ -1145,6 +1145,7 @@ struct SweepS8 {
 // __syncthreads.  Not used with rke (its correction needs the raw fluxes).
 struct SweepZ678 {
     enum { FE1, FE2, CV2N, RVN, DMN, V1S, FM1, FM2, FM3, NARR };
+    static constexpr int kThreads = 288;  // threads per block; lines of nz+4 threads each
 
     // SweepS6<2> at (i, j, k), k = -2..nz+1; returns the new rho (or 0).
     template <bool GEO>

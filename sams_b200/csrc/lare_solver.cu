@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kThreads, (MinBlocks<Op, P2>::value)) k_op(Ctx
 // The z sweep's stages S6, S7 and S8 (ops::SweepZ678) over whole z lines:
 // a block holds kZThreads / (nz + 4) lines of (i, j) in 0..nx x 0..ny, one
 // thread per k = -2..nz+1 of each.
-constexpr int kZThreads = 288;
+constexpr int kZThreads = ops::SweepZ678::kThreads;
 
 template <bool GEO>
 __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per SM, tuned on B200
