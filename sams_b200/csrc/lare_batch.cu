@@ -105,12 +105,12 @@ __global__ void __launch_bounds__(kT, (MinBlocksBatch<ops::Visc, P2>::value))
 // kThreads / (nz + 4) of them, starting at line p0 of (i, j) in
 // 0..nx x 0..ny.
 template <bool GEO>
-__global__ void __launch_bounds__(ops::SweepZ678::kThreads, 4)
+__global__ void __launch_bounds__(ops::kZLineThreads, 4)
     kb_zsweep(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles)
 {
     __shared__ Ctx c;
     extern __shared__ double zsm[];
-    constexpr int kZT = ops::SweepZ678::kThreads;
+    constexpr int kZT = ops::kZLineThreads;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const Tile tl = tiles[t];
         __syncthreads();
@@ -122,13 +122,13 @@ __global__ void __launch_bounds__(ops::SweepZ678::kThreads, 4)
         const long long q = (long long)tl.p0 + line;
         const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
         const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
-        const int at = line * W + k + 2;
-        double rho_new = 0.0;
-        if (on) rho_new = ops::SweepZ678::stage_a<GEO>(c, i, j, k, zsm, at, S);
+        using F = ops::SweepFused<2>;
+        const ops::LineStore st{zsm, S, line * W + k + 2};
+        if (on) F::stage_a<GEO>(c, i, j, k, st);
         __syncthreads();
-        if (on && k >= -1 && k <= g.nz) ops::SweepZ678::stage_b<GEO>(c, i, j, k, zsm, at, S, rho_new);
+        if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st);
         __syncthreads();
-        if (on && k >= 0 && k <= g.nz) ops::SweepZ678::stage_c(c, i, j, k, zsm, at, S);
+        if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st);
     }
 }
 
@@ -540,7 +540,7 @@ int Batch::rebuild()
     ntiles_ = (int)tiles.size();
     // z-line tiles of the fused z sweep, after the plane tiles; used when no
     // solve needs the raw momentum fluxes (rke) and every z line fits a block
-    constexpr int kZT = ops::SweepZ678::kThreads;
+    constexpr int kZT = ops::kZLineThreads;
     zfuse_ = nlive_ > 0 && !has_rke_;
     for (int q : live)
         if (slots_[q].ctx.g.nz + 4 > kZT) zfuse_ = false;
@@ -622,9 +622,9 @@ void Batch::launch(int arg, bool resistive_only)
 void Batch::launch_zsweep()
 {
     if (nztiles_ == 0) return;
-    constexpr int kZT = ops::SweepZ678::kThreads;
+    constexpr int kZT = ops::kZLineThreads;
     const int grid = std::min(nztiles_, sm_count_ * 4);
-    const size_t smem = (size_t)ops::SweepZ678::NARR * kZT * sizeof(double);
+    const size_t smem = (size_t)ops::SweepFused<2>::NARR * kZT * sizeof(double);
     if (has_geo_)
         kb_zsweep<true><<<grid, kZT, smem, stream_>>>(d_ctx_, d_tiles_ + ntiles_, nztiles_);
     else

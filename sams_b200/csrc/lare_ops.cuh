@@ -1134,102 +1134,120 @@ struct SweepS8 {
     }
 };
 
-// The z sweep's SweepS6, SweepS7 and SweepS8 as three stages of one kernel
-// (k_zsweep) over whole z lines.  Every value one stage passes to the next
-// is read only along z, on the same (i, j) line, so a block that holds whole
-// lines keeps them in shared memory: the energy fluxes, node cv2, vertex
-// density, node dm and shifted v1 of stage A and the momentum fluxes of
-// stage B never go to global memory.  Each stage is the same arithmetic as
-// the separate kernel it replaces.  Shared arrays are indexed by k + 2 from
-// the line's base (k = -2 .. nz+1); the kernel separates the stages with
-// __syncthreads.  Not used with rke (its correction needs the raw fluxes).
-struct SweepZ678 {
-    enum { FE1, FE2, CV2N, RVN, DMN, V1S, FM1, FM2, FM3, NARR };
-    static constexpr int kThreads = 288;  // threads per block; lines of nz+4 threads each
+// SweepS6, SweepS7 and SweepS8 of one sweep as three stages of one kernel.
+// Every value a stage passes to the next (energy fluxes, vertex density,
+// node dm, momentum fluxes) is read only along the sweep direction on the
+// same line, and every array the stages write (rho, energies, velocities)
+// is read only along that line too.  So a block that holds whole lines runs
+// the stages over them with __syncthreads in between and keeps those
+// intermediates in shared memory.  Used for the z sweep (k_zsweep,
+// kb_zsweep: lines along z, one thread per k), where a line is contiguous
+// in memory.  The arithmetic of each stage is the separate kernel's; node
+// cv2 and the shifted v1 are formed where they are used (same expressions).
+// Not used with rke (its correction needs the raw momentum fluxes in memory).
+// A is the intermediate store at one point: get(array, ds) reads it ds
+// points along the sweep, put(array, v) writes it here.
+template <int DIR>
+struct SweepFused {
+    enum { FE1, FE2, RVN, DMN, FM1, FM2, FM3, NARR };
 
-    // SweepS6<2> at (i, j, k), k = -2..nz+1; returns the new rho (or 0).
-    template <bool GEO>
-    __device__ static double stage_a(const Ctx &c, int i, int j, int k, double *sm, int at, int S)
+    // SweepS6 at (i, j, k), sweep index -2..n+1.
+    template <bool GEO, class A>
+    __device__ static void stage_a(const Ctx &c, int i, int j, int k, A b)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
         const RO dm{c.f[SAMS_F_DM]};
-        double rho_new = 0.0;
-        if (i >= 1 && j >= 1 && k >= 1 && k <= g.nz) {
-            rho_new = (rho1[o] * cv1[o] + dm[o - 1] - dm[o]) / cv2[o];
-            c.f[SAMS_F_RHO][o] = rho_new;
-        }
-        if (k >= 0 && k <= g.nz) {
-            double v = face_velocity<2>(c, o);
-            double area = face_area<2, GEO>(c, i, j, k);
+        const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+        const int qd = DIR == 0 ? i : (DIR == 1 ? j : k);
+        if (i >= 1 && j >= 1 && k >= 1 && i <= g.nx && j <= g.ny && k <= g.nz)
+            c.f[SAMS_F_RHO][o] = (rho1[o] * cv1[o] + dm[o - d] - dm[o]) / cv2[o];
+        if (qd >= 0 && qd <= nd) {  // the lines are 0..n across the sweep
+            double v = face_velocity<DIR>(c, o);
+            double area = face_area<DIR, GEO>(c, i, j, k);
             const RO ee{c.f[SAMS_F_ENERGY_ELECTRON]}, ei{c.f[SAMS_F_ENERGY_ION]};
-            sm[FE1 * S + at] = energy_flux(v, dt, area, ee[o - 1], ee[o], ee[o + 1], ee[o + 2], cvc1[o], cvc1[o - 1],
-                                           cvc1[o + 1], cv1[o], cv1[o + 1], rho1[o], rho1[o + 1], dm[o]);
-            sm[FE2 * S + at] = energy_flux(v, dt, area, ei[o - 1], ei[o], ei[o + 1], ei[o + 2], cvc1[o], cvc1[o - 1],
-                                           cvc1[o + 1], cv1[o], cv1[o + 1], rho1[o], rho1[o + 1], dm[o]);
-            sm[CV2N * S + at] = (cv2[o] + cv2[o + SX] + cv2[o + SY] + cv2[o + SX + SY] + cv2[o + 1] + cv2[o + SX + 1] +
-                                 cv2[o + SY + 1] + cv2[o + SX + SY + 1]) * 0.125;
+            b.put(FE1, energy_flux(v, dt, area, ee[o - d], ee[o], ee[o + d], ee[o + 2 * d], cvc1[o], cvc1[o - d],
+                                   cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]));
+            b.put(FE2, energy_flux(v, dt, area, ei[o - d], ei[o], ei[o + d], ei[o + 2 * d], cvc1[o], cvc1[o - d],
+                                   cvc1[o + d], cv1[o], cv1[o + d], rho1[o], rho1[o + d], dm[o]));
         }
-        if (k >= -1) {
+        if (qd >= -1) {
             double sum = rho1[o] * cv1[o] + rho1[o + SX] * cv1[o + SX] + rho1[o + SY] * cv1[o + SY] +
                          rho1[o + SX + SY] * cv1[o + SX + SY] + rho1[o + 1] * cv1[o + 1] +
                          rho1[o + SX + 1] * cv1[o + SX + 1] + rho1[o + SY + 1] * cv1[o + SY + 1] +
                          rho1[o + SX + SY + 1] * cv1[o + SX + SY + 1];
-            sm[RVN * S + at] = sum * (0.125 / cvc1[o]);
+            b.put(RVN, DIR == 0 ? sum * 0.125 / cvc1[o] : sum * (0.125 / cvc1[o]));
         }
-        if (k >= -1 && k <= g.nz)
-            sm[DMN * S + at] = (dm[o] + dm[o + SX] + dm[o + SY] + dm[o + SX + SY] + dm[o + 1] + dm[o + SX + 1] +
-                                dm[o + SY + 1] + dm[o + SX + SY + 1]) * 0.125;
-        const RO v1{c.f[SAMS_F_VZ1]};
-        sm[V1S * S + at] = (v1[o] + v1[o + 1]) * 0.5;
-        return rho_new;
+        if (qd >= -1 && qd <= nd)
+            b.put(DMN, (dm[o] + dm[o + SX] + dm[o + SY] + dm[o + SX + SY] + dm[o + 1] + dm[o + SX + 1] +
+                        dm[o + SY + 1] + dm[o + SX + SY + 1]) * 0.125);
     }
 
-    // SweepS7<2> at (i, j, k), k = -1..nz.
-    template <bool GEO>
-    __device__ static void stage_b(const Ctx &c, int i, int j, int k, double *sm, int at, int S, double rho_new)
+    // SweepS7 at (i, j, k), sweep index -1..n (after stage A everywhere).
+    template <bool GEO, class A>
+    __device__ static void stage_b(const Ctx &c, int i, int j, int k, A b)
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
         if (i >= 1 && j >= 1 && k >= 1) {
             double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
-            double den = cv2[o] * rho_new;
-            ee[o] = (ee[o] * cv1[o] * rho1[o] + sm[FE1 * S + at - 1] - sm[FE1 * S + at]) / den;
-            ei[o] = (ei[o] * cv1[o] * rho1[o] + sm[FE2 * S + at - 1] - sm[FE2 * S + at]) / den;
+            double den = cv2[o] * c.f[SAMS_F_RHO][o];  // stage A's rho (a coherent load)
+            ee[o] = (ee[o] * cv1[o] * rho1[o] + b.get(FE1, -1) - b.get(FE1, 0)) / den;
+            ei[o] = (ei[o] * cv1[o] * rho1[o] + b.get(FE2, -1) - b.get(FE2, 0)) / den;
         }
-        double area = dyac_at<GEO>(c, i, j, k);  // the z sweep uses dyac (zremap.cpp:475)
-        const double v = sm[V1S * S + at], dmv = sm[DMN * S + at];
-        const double dci = cv1[o + 1], dcm = cv1[o], dcp = cv1[o + 2], cvi = cvc1[o], cvp = cvc1[o + 1];
-        const double rvi = sm[RVN * S + at], rvp = sm[RVN * S + at + 1];
+        // x sweep uses dxac; the y and z sweeps both use dyac (zremap.cpp:475)
+        double area = DIR == 0 ? dxac_at<GEO>(c, i, j, k) : dyac_at<GEO>(c, i, j, k);
+        const RO v1{c.f[SAMS_F_VX1 + DIR]};
+        const double v = (v1[o] + v1[o + d]) * 0.5, dmv = b.get(DMN, 0);
+        const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
+        const double rvi = b.get(RVN, 0), rvp = b.get(RVN, 1);
         const RO ux{c.f[SAMS_F_VX]}, uy{c.f[SAMS_F_VY]}, uz{c.f[SAMS_F_VZ]};
-        const double f1 = mom_flux<true>(v, dt, area, ux[o - 1], ux[o], ux[o + 1], ux[o + 2], dci, dcm, dcp, cvi, cvp,
-                                         rvi, rvp, dmv);
-        const double f2 = mom_flux<true>(v, dt, area, uy[o - 1], uy[o], uy[o + 1], uy[o + 2], dci, dcm, dcp, cvi, cvp,
-                                         rvi, rvp, dmv);
-        const double f3 = mom_flux<true>(v, dt, area, uz[o - 1], uz[o], uz[o + 1], uz[o + 2], dci, dcm, dcp, cvi, cvp,
-                                         rvi, rvp, dmv);
-        sm[FM1 * S + at] = f1 * dmv;
-        sm[FM2 * S + at] = f2 * dmv;
-        sm[FM3 * S + at] = f3 * dmv;
+        const double f1 = mom_flux<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        const double f2 = mom_flux<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        const double f3 = mom_flux<DIR == 2>(v, dt, area, uz[o - d], uz[o], uz[o + d], uz[o + 2 * d], dci, dcm, dcp,
+                                             cvi, cvp, rvi, rvp, dmv);
+        b.put(FM1, f1 * dmv);
+        b.put(FM2, f2 * dmv);
+        b.put(FM3, f3 * dmv);
     }
 
-    // SweepS8<2> at (i, j, k), k = 0..nz.
-    __device__ static void stage_c(const Ctx &c, int i, int j, int k, const double *sm, int at, int S)
+    // SweepS8 at (i, j, k), sweep index 0..n (after stage B everywhere).
+    template <class A>
+    __device__ static void stage_c(const Ctx &c, int i, int j, int k, A b)
     {
         const Geom &g = c.g;
-        const int o = LOFF(i, j, k);
-        const double rvo = sm[RVN * S + at], cvco = __ldg(c.s[S_R_CVC1] + o), cv2o = sm[CV2N * S + at];
-        const double rho_v1 = (rvo * cvco + sm[DMN * S + at - 1] - sm[DMN * S + at]) / cv2o;
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const RO cv2{c.s[S_R_CV2]};
+        const double cv2o = (cv2[o] + cv2[o + SX] + cv2[o + SY] + cv2[o + SX + SY] + cv2[o + 1] + cv2[o + SX + 1] +
+                             cv2[o + SY + 1] + cv2[o + SX + SY + 1]) * 0.125;
+        const double rvo = b.get(RVN, 0), cvco = __ldg(c.s[S_R_CVC1] + o);
+        const double rho_v1 = (rvo * cvco + b.get(DMN, -1) - b.get(DMN, 0)) / cv2o;
         const double den = cv2o * rho_v1;
         double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
-        ux[o] = (rvo * ux[o] * cvco + sm[FM1 * S + at - 1] - sm[FM1 * S + at]) / den;
-        uy[o] = (rvo * uy[o] * cvco + sm[FM2 * S + at - 1] - sm[FM2 * S + at]) / den;
-        uz[o] = (rvo * uz[o] * cvco + sm[FM3 * S + at - 1] - sm[FM3 * S + at]) / den;
+        ux[o] = (rvo * ux[o] * cvco + b.get(FM1, -1) - b.get(FM1, 0)) / den;
+        uy[o] = (rvo * uy[o] * cvco + b.get(FM2, -1) - b.get(FM2, 0)) / den;
+        uz[o] = (rvo * uz[o] * cvco + b.get(FM3, -1) - b.get(FM3, 0)) / den;
     }
+};
+
+// Threads per block of the fused z sweep: whole z lines of nz+4 threads.
+constexpr int kZLineThreads = 288;
+
+// Intermediates of the block's z lines: array a at sm[a * S + at], at =
+// line base + k + 2.
+struct LineStore {
+    double *sm;
+    int S, at;
+    __device__ double get(int a, int ds) const { return sm[a * S + at + ds]; }
+    __device__ void put(int a, double v) const { sm[a * S + at] = v; }
 };
 
 // ---------------------------------------------------------------------------

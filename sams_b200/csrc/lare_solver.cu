@@ -45,14 +45,15 @@ __global__ void __launch_bounds__(kThreads, (MinBlocks<Op, P2>::value)) k_op(Ctx
     for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) Op::template run<GEO, P2>(c, arg, i, j, k);
 }
 
-// The z sweep's stages S6, S7 and S8 (ops::SweepZ678) over whole z lines:
-// a block holds kZThreads / (nz + 4) lines of (i, j) in 0..nx x 0..ny, one
-// thread per k = -2..nz+1 of each.
-constexpr int kZThreads = ops::SweepZ678::kThreads;
+// The z sweep's stages S6, S7 and S8 (ops::SweepFused<2>) over whole z
+// lines: a block holds kZThreads / (nz + 4) lines of (i, j) in 0..nx x
+// 0..ny, one thread per k = -2..nz+1 of each.
+constexpr int kZThreads = ops::kZLineThreads;
 
 template <bool GEO>
 __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per SM, tuned on B200
 {
+    using F = ops::SweepFused<2>;
     extern __shared__ double zsm[];
     const Geom &g = c.g;
     const int W = g.nz + 4, lines = kZThreads / W, S = lines * W;
@@ -60,13 +61,12 @@ __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per
     const long long q = (long long)blockIdx.x * lines + line;
     const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
     const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
-    const int at = line * W + k + 2;
-    double rho_new = 0.0;
-    if (on) rho_new = ops::SweepZ678::stage_a<GEO>(c, i, j, k, zsm, at, S);
+    const ops::LineStore st{zsm, S, line * W + k + 2};
+    if (on) F::stage_a<GEO>(c, i, j, k, st);
     __syncthreads();
-    if (on && k >= -1 && k <= g.nz) ops::SweepZ678::stage_b<GEO>(c, i, j, k, zsm, at, S, rho_new);
+    if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st);
     __syncthreads();
-    if (on && k >= 0 && k <= g.nz) ops::SweepZ678::stage_c(c, i, j, k, zsm, at, S);
+    if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st);
 }
 
 // Visc with the CFL minimum: each block reduces its candidates and folds
@@ -673,7 +673,7 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         const Geom &g = ctx_.g;
         const int W = g.nz + 4, lines = kZThreads / W;
         const long long nl = (long long)(g.nx + 1) * (g.ny + 1);
-        const size_t smem = (size_t)ops::SweepZ678::NARR * lines * W * sizeof(double);
+        const size_t smem = (size_t)ops::SweepFused<2>::NARR * lines * W * sizeof(double);
         const unsigned blocks = (unsigned)ceil_div(nl, lines);
         if (ctx_.p.geometry)
             k_zsweep<true><<<blocks, kZThreads, smem, stream_>>>(ctx_);
