@@ -124,11 +124,12 @@ __global__ void __launch_bounds__(ops::kZLineThreads, 4)
         const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
         using F = ops::SweepFused<2>;
         const ops::LineStore st{zsm, S, line * W + k + 2};
-        if (on) F::stage_a<GEO>(c, i, j, k, st);
+        const ops::SweepOut w = ops::sweep_in_place(c);
+        if (on) F::stage_a<GEO>(c, i, j, k, st, w, true);
         __syncthreads();
-        if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st);
+        if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st, w, true);
         __syncthreads();
-        if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st);
+        if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st, w);
     }
 }
 

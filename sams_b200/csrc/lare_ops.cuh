@@ -1134,17 +1134,35 @@ struct SweepS8 {
     }
 };
 
+// The state arrays a fused sweep writes: in place (the solve's own rho,
+// energies and velocities) or into six free scratch arrays (x and y sweeps,
+// see k_psweep), in which case the solve's arrays are only read.
+struct SweepOut {
+    double *rho, *ee, *ei, *ux, *uy, *uz;
+};
+
+__device__ __forceinline__ SweepOut sweep_in_place(const Ctx &c)
+{
+    return SweepOut{c.f[SAMS_F_RHO], c.f[SAMS_F_ENERGY_ELECTRON], c.f[SAMS_F_ENERGY_ION],
+                    c.f[SAMS_F_VX], c.f[SAMS_F_VY], c.f[SAMS_F_VZ]};
+}
+
 // SweepS6, SweepS7 and SweepS8 of one sweep as three stages of one kernel.
 // Every value a stage passes to the next (energy fluxes, vertex density,
 // node dm, momentum fluxes) is read only along the sweep direction on the
-// same line, and every array the stages write (rho, energies, velocities)
-// is read only along that line too.  So a block that holds whole lines runs
-// the stages over them with __syncthreads in between and keeps those
-// intermediates in shared memory.  Used for the z sweep (k_zsweep,
-// kb_zsweep: lines along z, one thread per k), where a line is contiguous
-// in memory.  The arithmetic of each stage is the separate kernel's; node
-// cv2 and the shifted v1 are formed where they are used (same expressions).
-// Not used with rke (its correction needs the raw momentum fluxes in memory).
+// same line, so a block that holds a stretch of lines runs the stages over
+// it with __syncthreads in between and keeps those intermediates in shared
+// memory:
+//   k_zsweep (z): whole z lines, one thread per k, in place (every array
+//     the stages write is read only along its own line);
+//   k_psweep (x, y): 32 adjacent z values x a window of the line plus a
+//     recomputed halo, writing rho, energies and velocities out of place
+//     (SweepOut), so no block reads a value another block has updated.
+// Stage A and B at halo points (own == false) compute the intermediates
+// only; the state is written at the window's own points.  The arithmetic of
+// each stage is the separate kernel's; node cv2 and the shifted v1 are formed
+// where they are used (same expressions).  Not used with rke (its correction
+// needs the raw momentum fluxes in memory).
 // A is the intermediate store at one point: get(array, ds) reads it ds
 // points along the sweep, put(array, v) writes it here.
 template <int DIR>
@@ -1153,7 +1171,7 @@ struct SweepFused {
 
     // SweepS6 at (i, j, k), sweep index -2..n+1.
     template <bool GEO, class A>
-    __device__ static void stage_a(const Ctx &c, int i, int j, int k, A b)
+    __device__ static void stage_a(const Ctx &c, int i, int j, int k, A b, const SweepOut &w, bool own)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
@@ -1163,8 +1181,8 @@ struct SweepFused {
         const RO dm{c.f[SAMS_F_DM]};
         const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
         const int qd = DIR == 0 ? i : (DIR == 1 ? j : k);
-        if (i >= 1 && j >= 1 && k >= 1 && i <= g.nx && j <= g.ny && k <= g.nz)
-            c.f[SAMS_F_RHO][o] = (rho1[o] * cv1[o] + dm[o - d] - dm[o]) / cv2[o];
+        if (own && i >= 1 && j >= 1 && k >= 1 && i <= g.nx && j <= g.ny && k <= g.nz)
+            w.rho[o] = (rho1[o] * cv1[o] + dm[o - d] - dm[o]) / cv2[o];
         if (qd >= 0 && qd <= nd) {  // the lines are 0..n across the sweep
             double v = face_velocity<DIR>(c, o);
             double area = face_area<DIR, GEO>(c, i, j, k);
@@ -1188,18 +1206,20 @@ struct SweepFused {
 
     // SweepS7 at (i, j, k), sweep index -1..n (after stage A everywhere).
     template <bool GEO, class A>
-    __device__ static void stage_b(const Ctx &c, int i, int j, int k, A b)
+    __device__ static void stage_b(const Ctx &c, int i, int j, int k, A b, const SweepOut &w, bool own)
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
         const int d = dir_stride(g, DIR);
         const double dt = c.sc->dt;
         const RO rho1{c.s[S_R_RHO1]}, cv1{c.s[S_R_CV1]}, cv2{c.s[S_R_CV2]}, cvc1{c.s[S_R_CVC1]};
-        if (i >= 1 && j >= 1 && k >= 1) {
-            double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
-            double den = cv2[o] * c.f[SAMS_F_RHO][o];  // stage A's rho (a coherent load)
-            ee[o] = (ee[o] * cv1[o] * rho1[o] + b.get(FE1, -1) - b.get(FE1, 0)) / den;
-            ei[o] = (ei[o] * cv1[o] * rho1[o] + b.get(FE2, -1) - b.get(FE2, 0)) / den;
+        if (own && i >= 1 && j >= 1 && k >= 1) {
+            const double *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
+            double den = cv2[o] * w.rho[o];  // stage A's rho (a coherent load)
+            const double e_new = (ee[o] * cv1[o] * rho1[o] + b.get(FE1, -1) - b.get(FE1, 0)) / den;
+            const double i_new = (ei[o] * cv1[o] * rho1[o] + b.get(FE2, -1) - b.get(FE2, 0)) / den;
+            w.ee[o] = e_new;
+            w.ei[o] = i_new;
         }
         // x sweep uses dxac; the y and z sweeps both use dyac (zremap.cpp:475)
         double area = DIR == 0 ? dxac_at<GEO>(c, i, j, k) : dyac_at<GEO>(c, i, j, k);
@@ -1207,7 +1227,7 @@ struct SweepFused {
         const double v = (v1[o] + v1[o + d]) * 0.5, dmv = b.get(DMN, 0);
         const double dci = cv1[o + d], dcm = cv1[o], dcp = cv1[o + 2 * d], cvi = cvc1[o], cvp = cvc1[o + d];
         const double rvi = b.get(RVN, 0), rvp = b.get(RVN, 1);
-        const RO ux{c.f[SAMS_F_VX]}, uy{c.f[SAMS_F_VY]}, uz{c.f[SAMS_F_VZ]};
+        const double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
         const double f1 = mom_flux<DIR == 2>(v, dt, area, ux[o - d], ux[o], ux[o + d], ux[o + 2 * d], dci, dcm, dcp,
                                              cvi, cvp, rvi, rvp, dmv);
         const double f2 = mom_flux<DIR == 2>(v, dt, area, uy[o - d], uy[o], uy[o + d], uy[o + 2 * d], dci, dcm, dcp,
@@ -1221,7 +1241,7 @@ struct SweepFused {
 
     // SweepS8 at (i, j, k), sweep index 0..n (after stage B everywhere).
     template <class A>
-    __device__ static void stage_c(const Ctx &c, int i, int j, int k, A b)
+    __device__ static void stage_c(const Ctx &c, int i, int j, int k, A b, const SweepOut &w)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
@@ -1231,10 +1251,13 @@ struct SweepFused {
         const double rvo = b.get(RVN, 0), cvco = __ldg(c.s[S_R_CVC1] + o);
         const double rho_v1 = (rvo * cvco + b.get(DMN, -1) - b.get(DMN, 0)) / cv2o;
         const double den = cv2o * rho_v1;
-        double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
-        ux[o] = (rvo * ux[o] * cvco + b.get(FM1, -1) - b.get(FM1, 0)) / den;
-        uy[o] = (rvo * uy[o] * cvco + b.get(FM2, -1) - b.get(FM2, 0)) / den;
-        uz[o] = (rvo * uz[o] * cvco + b.get(FM3, -1) - b.get(FM3, 0)) / den;
+        const double *ux = c.f[SAMS_F_VX], *uy = c.f[SAMS_F_VY], *uz = c.f[SAMS_F_VZ];
+        const double nx = (rvo * ux[o] * cvco + b.get(FM1, -1) - b.get(FM1, 0)) / den;
+        const double ny = (rvo * uy[o] * cvco + b.get(FM2, -1) - b.get(FM2, 0)) / den;
+        const double nz = (rvo * uz[o] * cvco + b.get(FM3, -1) - b.get(FM3, 0)) / den;
+        w.ux[o] = nx;
+        w.uy[o] = ny;
+        w.uz[o] = nz;
     }
 };
 
@@ -1248,6 +1271,19 @@ struct LineStore {
     int S, at;
     __device__ double get(int a, int ds) const { return sm[a * S + at + ds]; }
     __device__ void put(int a, double v) const { sm[a * S + at] = v; }
+};
+
+// Fused x / y sweep windows: kWinK adjacent z values (a warp) x kWinS own
+// points along the line, plus stage A's halo of two points before and one
+// after and stage B's of one before.  Array a of the window at
+// sm[((a * P) + p) * kWinK + kc], p = s - s0 + 2, P = kWinS + 3.
+constexpr int kWinK = 32, kWinS = 24, kWinThreads = 256;  // 48 KB of shared memory: 4 blocks per SM
+struct WinStore {
+    double *sm;
+    int at, kc;
+    static constexpr int P = kWinS + 3;
+    __device__ double get(int a, int ds) const { return sm[(a * P + at + ds) * kWinK + kc]; }
+    __device__ void put(int a, double v) const { sm[(a * P + at) * kWinK + kc] = v; }
 };
 
 // ---------------------------------------------------------------------------

@@ -62,11 +62,73 @@ __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per
     const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
     const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
     const ops::LineStore st{zsm, S, line * W + k + 2};
-    if (on) F::stage_a<GEO>(c, i, j, k, st);
+    const ops::SweepOut w = ops::sweep_in_place(c);
+    if (on) F::stage_a<GEO>(c, i, j, k, st, w, true);
     __syncthreads();
-    if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st);
+    if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st, w, true);
     __syncthreads();
-    if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st);
+    if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st, w);
+}
+
+// The x or y sweep's stages (ops::SweepFused<DIR>) out of place, over
+// windows of kWinK adjacent k in 0..nz times kWinS own points along DIR, for
+// one value of the third index (j for x, i for y) in 0..n.  The solve's
+// state arrays are only read; the new rho, energies and velocities go to w.
+// Halo points recompute stage A (two before, one after) and stage B (one
+// before) without writing the state.
+template <int DIR, bool GEO>
+__global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::SweepOut w)  // window shape and cap tuned on B200
+{
+    using F = ops::SweepFused<DIR>;
+    constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
+    extern __shared__ double psm[];
+    const Geom &g = c.g;
+    const int nd = DIR == 0 ? g.nx : g.ny;
+    const int nkt = (g.nz + TK) / TK, nwin = (nd + ops::kWinS) / ops::kWinS;
+    const int b = (int)blockIdx.x;
+    const int win = b % nwin, kt = (b / nwin) % nkt, a = b / (nwin * nkt);
+    const int s0 = win * ops::kWinS, s1 = min(s0 + ops::kWinS - 1, nd);  // own points
+    const int kc = (int)threadIdx.x % TK, sl = (int)threadIdx.x / TK;
+    const int k = kt * TK + kc;
+    const bool on = k <= g.nz;
+    auto at = [&](int s) { return ops::WinStore{psm, s - s0 + 2, kc}; };
+    const int a_lo = max(s0 - 2, -2), a_hi = min(s1 + 1, nd + 1);
+    for (int s = a_lo + sl; s <= a_hi; s += TS)
+        if (on) F::template stage_a<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w, s >= s0 && s <= s1);
+    __syncthreads();
+    const int b_lo = max(s0 - 1, -1);
+    for (int s = b_lo + sl; s <= s1; s += TS)
+        if (on) F::template stage_b<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w, s >= s0);
+    __syncthreads();
+    for (int s = s0 + sl; s <= s1; s += TS)
+        if (on) F::stage_c(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w);
+}
+
+// The points of the out-of-place sweep's arrays it does not compute (rho and
+// energies outside 1..n, velocities outside 0..n in some dimension): copied
+// from the solve's arrays, so the new arrays are complete boxes.
+__global__ void __launch_bounds__(kThreads) k_copy_shell(Ctx c, ops::SweepOut w)
+{
+    const Geom &g = c.g;
+    const long long ey = g.ny + 5, ez = g.nz + 5;
+    const long long n = (long long)(g.nx + 5) * ey * ez;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / (ey * ez)) - 2, j = (int)((t / ez) % ey) - 2, k = (int)(t % ez) - 2;
+        const int o = box_off(g, i, j, k);
+        const bool cell = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
+        const bool node = i >= 0 && i <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
+        if (!cell) {
+            w.rho[o] = c.f[SAMS_F_RHO][o];
+            w.ee[o] = c.f[SAMS_F_ENERGY_ELECTRON][o];
+            w.ei[o] = c.f[SAMS_F_ENERGY_ION][o];
+        }
+        if (!node) {
+            w.ux[o] = c.f[SAMS_F_VX][o];
+            w.uy[o] = c.f[SAMS_F_VY][o];
+            w.uz[o] = c.f[SAMS_F_VZ][o];
+        }
+    }
 }
 
 // Visc with the CFL minimum: each block reduces its candidates and folds
@@ -396,6 +458,7 @@ int Solver::init_impl(const sams_lare_params &p, const sams_lare_bcs &bcs, int d
     if ((rc = check(cudaMemcpy(sc_, &s0, sizeof(s0), cudaMemcpyHostToDevice), "scalars upload"))) return rc;
     ctx_.sc = sc_;
     bytes_ = (long long)abytes + (long long)(packed.size() * sizeof(double)) + (long long)sizeof(Scalars);
+    if ((rc = setup_psweep())) return rc;
     return check(cudaStreamSynchronize(stream_), "init sync");
 }
 
@@ -423,7 +486,7 @@ int Solver::init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, c
     ctx_ = ctx;
     sc_ = ctx.sc;  // borrowed: release_borrowed() must clear it before destruction
     stream_ = stream;
-    return SAMS_OK;
+    return setup_psweep();
 }
 
 void Solver::release_borrowed()
@@ -510,6 +573,52 @@ int Solver::download(int field, double *dst, cudaMemcpyKind kind)
     }
     if (rc) return rc;
     return check(cudaStreamSynchronize(stream_), "download sync");
+}
+
+// The x or y sweep's S6-S8 out of place into six scratch arrays free during
+// the remap (the intermediates of the separate kernels live on chip here),
+// then the solve's state pointers move to them; the y sweep writes back into
+// the arrays the x sweep left, so after the two sweeps every pointer is
+// where it started.
+template <int DIR>
+void Solver::launch_psweep()
+{
+    static const int kOut[6] = {S_FX, S_FY, S_FZ, S_VH, S_FXV, S_FYV};
+    static const int kState[6] = {SAMS_F_RHO, SAMS_F_ENERGY_ELECTRON, SAMS_F_ENERGY_ION,
+                                  SAMS_F_VX, SAMS_F_VY, SAMS_F_VZ};
+    const Geom &g = ctx_.g;
+    const ops::SweepOut w{ctx_.s[kOut[0]], ctx_.s[kOut[1]], ctx_.s[kOut[2]],
+                          ctx_.s[kOut[3]], ctx_.s[kOut[4]], ctx_.s[kOut[5]]};
+    const int nd = DIR == 0 ? g.nx : g.ny, na = (DIR == 0 ? g.ny : g.nx) + 1;
+    const long long blocks = (long long)na * ((g.nz + ops::kWinK) / ops::kWinK) * ((nd + ops::kWinS) / ops::kWinS);
+    const size_t smem = (size_t)ops::SweepFused<DIR>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
+    if (ctx_.p.geometry)
+        k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
+    else
+        k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
+    const long long box = (long long)(g.nx + 5) * (g.ny + 5) * (g.nz + 5);
+    k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(box, kThreads), 8L * sm_count_), kThreads, 0, stream_>>>(ctx_, w);
+    launches_ += 2;
+    for (int q = 0; q < 6; ++q) std::swap(ctx_.f[kState[q]], ctx_.s[kOut[q]]);
+}
+
+// The fused x / y sweep needs more than the default 48 KB of shared memory
+// per block; allow the device's opt-in maximum (the attribute belongs to
+// the kernel, so it is the same for every solve).
+int Solver::setup_psweep()
+{
+    int maxsm = 0, rc;
+    if ((rc = check(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_), "smem limit")))
+        return rc;
+    const size_t need = (size_t)ops::SweepFused<0>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
+    psweep_ok_ = need <= (size_t)maxsm;
+    if (!psweep_ok_) return SAMS_OK;
+    const void *fn[4] = {(const void *)k_psweep<0, false>, (const void *)k_psweep<0, true>,
+                         (const void *)k_psweep<1, false>, (const void *)k_psweep<1, true>};
+    for (const void *f : fn)
+        if ((rc = check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm), "psweep smem")))
+            return rc;
+    return SAMS_OK;
 }
 
 template <class Op>
@@ -639,13 +748,17 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     launch<ops::SweepCTUpd<0>>(0);
     launch<ops::SweepMass<0>>(0);
     bc_fill_dim(FM_DM, 0);
-    launch<ops::SweepS6<0>>(0);
-    launch<ops::SweepS7<0>>(0);
-    if (p_.rke) {
-        launch<ops::SweepRkeDk<0>>(0);
-        launch<ops::SweepRkeGather<0>>(0);
+    if (!p_.rke && psweep_ok_) {
+        launch_psweep<0>();
+    } else {
+        launch<ops::SweepS6<0>>(0);
+        launch<ops::SweepS7<0>>(0);
+        if (p_.rke) {
+            launch<ops::SweepRkeDk<0>>(0);
+            launch<ops::SweepRkeGather<0>>(0);
+        }
+        launch<ops::SweepS8<0>>(0);
     }
-    launch<ops::SweepS8<0>>(0);
     bc_fill(FM_ALL9);
     mark(3);
     launch<ops::SweepVol<1>>(0);
@@ -654,13 +767,17 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     launch<ops::SweepCTUpd<1>>(0);
     launch<ops::SweepMass<1>>(0);
     bc_fill_dim(FM_DM, 1);
-    launch<ops::SweepS6<1>>(0);
-    launch<ops::SweepS7<1>>(0);
-    if (p_.rke) {
-        launch<ops::SweepRkeDk<1>>(0);
-        launch<ops::SweepRkeGather<1>>(0);
+    if (!p_.rke && psweep_ok_) {
+        launch_psweep<1>();
+    } else {
+        launch<ops::SweepS6<1>>(0);
+        launch<ops::SweepS7<1>>(0);
+        if (p_.rke) {
+            launch<ops::SweepRkeDk<1>>(0);
+            launch<ops::SweepRkeGather<1>>(0);
+        }
+        launch<ops::SweepS8<1>>(0);
     }
-    launch<ops::SweepS8<1>>(0);
     bc_fill(FM_ALL9);
     mark(4);
     launch<ops::SweepVol<2>>(0);

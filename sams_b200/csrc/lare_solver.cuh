@@ -107,6 +107,8 @@ private:
     void bc_fill_dim(unsigned mask, int dim);
     bool all_periodic(unsigned mask) const;
     template <class Op> void launch(int arg);
+    template <int DIR> void launch_psweep();
+    int setup_psweep();
     int staging(double **out);
     void free_all();
 
@@ -115,6 +117,7 @@ private:
     sams_lare_params p_{};
     BcTable bc_{};
     Halo *halo_ = nullptr;
+    bool psweep_ok_ = false;  // the fused x / y sweep's shared memory fits this device
     int device_ = 0;
     int sm_count_ = 148;  // multiprocessors of device_ (grid sizing)
     cudaStream_t own_stream_ = nullptr;
