@@ -602,16 +602,20 @@ void Solver::launch_psweep()
     for (int q = 0; q < 6; ++q) std::swap(ctx_.f[kState[q]], ctx_.s[kOut[q]]);
 }
 
-// The fused x / y sweep needs more than the default 48 KB of shared memory
-// per block; allow the device's opt-in maximum (the attribute belongs to
-// the kernel, so it is the same for every solve).
+// Whether the fused x / y sweep runs for this solve (its windows must be at
+// least three quarters full of k values), and its shared memory: allow the
+// device's opt-in maximum (the attribute belongs to the kernel, so it is
+// the same for every solve).
 int Solver::setup_psweep()
 {
     int maxsm = 0, rc;
     if ((rc = check(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_), "smem limit")))
         return rc;
     const size_t need = (size_t)ops::SweepFused<0>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
-    psweep_ok_ = need <= (size_t)maxsm;
+    // a window holds kWinK adjacent k; thin grids would leave most lanes idle
+    const int kw = ops::kWinK, nk = ctx_.g.nz + 1;
+    const bool lanes_full = 4 * nk >= 3 * kw * ((nk + kw - 1) / kw);
+    psweep_ok_ = need <= (size_t)maxsm && lanes_full;
     if (!psweep_ok_) return SAMS_OK;
     const void *fn[4] = {(const void *)k_psweep<0, false>, (const void *)k_psweep<0, true>,
                          (const void *)k_psweep<1, false>, (const void *)k_psweep<1, true>};

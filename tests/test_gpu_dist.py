@@ -53,6 +53,8 @@ def _assert_equal(one, dist, n, label):
     ("ot", (12, 10, 6), 2, 4, {"geometry": 1, "domain": GEO_DOMAIN}),
     ("rf", (12, 8, 6), 2, 3, {"geometry": 2, "domain": GEO_DOMAIN}),
     ("rf", (64, 32, 32), 4, 3, None),
+    ("rf", (12, 8, 24), 3, 3, None),               # fused out-of-place x / y sweeps
+    ("ot", (10, 8, 24), 2, 3, {"geometry": 1, "domain": GEO_DOMAIN}),
 ])
 def test_slabs_equal_undivided_solve(case, n, parts, steps, opts):
     one, dist = _pair(case, n, parts, options=opts)

@@ -58,6 +58,10 @@ def test_gpu_matches_reference_golden(name):
     ("rf", (8, 8, 2), 5),          # fewer than three cells in z: ordered edge copies
     ("ot", (2, 9, 5), 5),          # ... in x
     ("harris", (12, 1, 6), 4),     # ... one cell in y, walls
+    # z lines long enough for the fused out-of-place x / y sweep kernel
+    ("rf", (12, 10, 24), 4),
+    ("harris", (10, 12, 28), 3),
+    ("ot", (9, 7, 26), 4),
 ])
 def test_gpu_matches_checker(case, n, steps, oracle_lib):
     lo = oracle_lib
@@ -167,7 +171,8 @@ def test_gpu_resistive_with_inconsistent_energy_ghosts(oracle_lib):
 
 
 @pytest.mark.parametrize("case,n,steps,geometry,rke", [("ot", (24, 20, 8), 6, 1, 0), ("rf", (16, 12, 10), 4, 2, 0),
-                                                       ("harris", (16, 12, 6), 4, 1, 1), ("rf", (12, 10, 2), 3, 2, 1)])
+                                                       ("harris", (16, 12, 6), 4, 1, 1), ("rf", (12, 10, 2), 3, 2, 1),
+                                                       ("rf", (10, 8, 24), 3, 2, 0), ("ot", (12, 8, 25), 3, 1, 0)])
 def test_gpu_matches_checker_in_curvilinear_geometry(case, n, steps, geometry, rke, oracle_lib):
     """Cylindrical and spherical geometry (metric factors on r in [1, 2],
     theta in [0.5, 1.5]) against the checker, bit for bit."""
