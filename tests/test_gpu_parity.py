@@ -62,6 +62,8 @@ def test_gpu_matches_reference_golden(name):
     ("rf", (12, 10, 24), 4),
     ("harris", (10, 12, 28), 3),
     ("ot", (9, 7, 26), 4),
+    ("ot", (2, 9, 24), 4),         # ... with fewer than three cells along the sweep
+    ("rf", (8, 2, 26), 3),
 ])
 def test_gpu_matches_checker(case, n, steps, oracle_lib):
     lo = oracle_lib
