@@ -35,6 +35,50 @@ __host__ __device__ inline int box_off(const Geom &g, int i, int j, int k)
     return (i + 2) * g.sx + (j + 2) * g.sy + (k + g.zoff);
 }
 
+// The points of a box (-2..n+2 in each dimension) outside the cube
+// lo..n+hi in every dimension, one per index t in 0 .. count()-1:
+// first the x slabs (whole y-z planes), then the y slabs inside the cube's
+// x range, then the z slabs inside its x and y ranges.
+struct BoxShell {
+    int n[3];
+    int lo, hi;
+    __host__ __device__ long long ext(int d) const { return (long long)n[d] + 5; }
+    __host__ __device__ long long in(int d) const { return (long long)n[d] + hi - lo + 1; }
+    // box index of the q-th ghost layer of dimension d (lo+2 below, the rest above)
+    __host__ __device__ int ghost(int d, long long q) const
+    {
+        return q < lo + 2 ? (int)q - 2 : n[d] + hi + 1 + (int)(q - (lo + 2));
+    }
+    __host__ __device__ long long count() const
+    {
+        return (ext(0) - in(0)) * ext(1) * ext(2) + in(0) * (ext(1) - in(1)) * ext(2) +
+               in(0) * in(1) * (ext(2) - in(2));
+    }
+    __host__ __device__ void point(long long t, int &i, int &j, int &k) const
+    {
+        const long long cx = (ext(0) - in(0)) * ext(1) * ext(2);
+        if (t < cx) {
+            i = ghost(0, t / (ext(1) * ext(2)));
+            j = (int)((t / ext(2)) % ext(1)) - 2;
+            k = (int)(t % ext(2)) - 2;
+            return;
+        }
+        t -= cx;
+        const long long gy = ext(1) - in(1), cy = in(0) * gy * ext(2);
+        if (t < cy) {
+            i = lo + (int)(t / (gy * ext(2)));
+            j = ghost(1, (t / ext(2)) % gy);
+            k = (int)(t % ext(2)) - 2;
+            return;
+        }
+        t -= cy;
+        const long long gz = ext(2) - in(2);
+        i = lo + (int)(t / (in(1) * gz));
+        j = lo + (int)((t / gz) % in(1));
+        k = ghost(2, t % gz);
+    }
+};
+
 // Staggering of a field in one dimension (1 = half cell), the device-side
 // copy of sams_lare_field_stagger.
 __host__ __device__ constexpr int field_half(int f, int d)

@@ -106,24 +106,25 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::Swee
 
 // The points of the out-of-place sweep's arrays it does not compute (rho and
 // energies outside 1..n, velocities outside 0..n in some dimension): copied
-// from the solve's arrays, so the new arrays are complete boxes.
+// from the solve's arrays, so the new arrays are complete boxes.  One
+// thread per shell point: the rho / energy shell, then the velocity shell.
 __global__ void __launch_bounds__(kThreads) k_copy_shell(Ctx c, ops::SweepOut w)
 {
     const Geom &g = c.g;
-    const long long ey = g.ny + 5, ez = g.nz + 5;
-    const long long n = (long long)(g.nx + 5) * ey * ez;
+    const BoxShell cell{{g.nx, g.ny, g.nz}, 1, 0}, node{{g.nx, g.ny, g.nz}, 0, 0};
+    const long long nc = cell.count(), n = nc + node.count();
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t / (ey * ez)) - 2, j = (int)((t / ez) % ey) - 2, k = (int)(t % ez) - 2;
-        const int o = box_off(g, i, j, k);
-        const bool cell = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
-        const bool node = i >= 0 && i <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
-        if (!cell) {
+        int i, j, k;
+        if (t < nc) {
+            cell.point(t, i, j, k);
+            const int o = box_off(g, i, j, k);
             w.rho[o] = c.f[SAMS_F_RHO][o];
             w.ee[o] = c.f[SAMS_F_ENERGY_ELECTRON][o];
             w.ei[o] = c.f[SAMS_F_ENERGY_ION][o];
-        }
-        if (!node) {
+        } else {
+            node.point(t - nc, i, j, k);
+            const int o = box_off(g, i, j, k);
             w.ux[o] = c.f[SAMS_F_VX][o];
             w.uy[o] = c.f[SAMS_F_VY][o];
             w.uz[o] = c.f[SAMS_F_VZ][o];
@@ -596,8 +597,8 @@ void Solver::launch_psweep()
         k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
     else
         k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
-    const long long box = (long long)(g.nx + 5) * (g.ny + 5) * (g.nz + 5);
-    k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(box, kThreads), 8L * sm_count_), kThreads, 0, stream_>>>(ctx_, w);
+    const long long shell = BoxShell{{g.nx, g.ny, g.nz}, 1, 0}.count() + BoxShell{{g.nx, g.ny, g.nz}, 0, 0}.count();
+    k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(shell, kThreads), 8L * sm_count_), kThreads, 0, stream_>>>(ctx_, w);
     launches_ += 2;
     for (int q = 0; q < 6; ++q) std::swap(ctx_.f[kState[q]], ctx_.s[kOut[q]]);
 }
