@@ -15,6 +15,32 @@ ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "_build", "liblare_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "lare_ref")
 REF_BENCH_BIN = os.path.join(HERE, "_ref", "lare_ref_bench")
+REF_BENCH_BIN_V4 = os.path.join(HERE, "_ref", "lare_ref_bench_v4")
+AVX512_V4 = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
+def host_isa():
+    """'x86-64-v4' when this host's CPU has the AVX-512 subsets of that level,
+    else 'x86-64-v3'."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = set()
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        return "x86-64-v3"
+    return "x86-64-v4" if all(x in flags for x in AVX512_V4) else "x86-64-v3"
+
+
+def reference_bench_binary():
+    """The reference's release build for the widest ISA this host runs (the
+    reference builds with -march=native), and that ISA."""
+    isa = host_isa()
+    if isa == "x86-64-v4" and os.path.exists(REF_BENCH_BIN_V4):
+        return REF_BENCH_BIN_V4, isa
+    return REF_BENCH_BIN, "x86-64-v3"
 
 NFIELDS = 13
 FIELD_NAMES = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz",
@@ -75,10 +101,24 @@ def lib():
     return _lib
 
 
-def build():
-    """Build the checker (and, where the reference tree exists, the
-    reference harness)."""
-    subprocess.run(["make", "-s", "-C", HERE, "-j8"], check=True)
+def build(ref_tree=None):
+    """Build the checker, and the reference harness when `ref_tree` (the
+    reference source tree; default: the SAMS_REFERENCE_TREE environment
+    variable) is given."""
+    ref_tree = ref_tree or os.environ.get("SAMS_REFERENCE_TREE")
+    cmd = ["make", "-s", "-C", HERE, "-j8"] + (["REF=" + ref_tree] if ref_tree else [])
+    subprocess.run(cmd, check=True)
+
+
+def reference_tree():
+    """The reference source tree the harness was last built from, or None
+    (recorded by oracle/Makefile; absent where the tree never was)."""
+    try:
+        with open(os.path.join(HERE, "_ref", "ref_tree.txt")) as f:
+            path = f.read().strip()
+    except OSError:
+        return None
+    return path if path and os.path.isdir(path) else None
 
 
 def box_shape(nx, ny, nz):

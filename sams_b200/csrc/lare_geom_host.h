@@ -102,7 +102,10 @@ inline void geom_bind(GeomF &gf, const double *dev, const sams_lare_params &p)
 // True when every spacing array (as the axis builders lay them out: index
 // i + 2, b over -2..n+2, c over -1..n+2) holds one value per axis, that
 // value is a power of two, and so is mu0; fills the reciprocals (exact for
-// powers of two).
+// powers of two).  Each of these values must lie in [2^-340, 2^340]: then
+// every product of up to three of them (a face area, a cell volume) is a
+// normal number and its reciprocal is finite and exact.  A subnormal spacing
+// is a power of two for frexp too, but its reciprocal overflows.
 inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> &dyb, const std::vector<double> &dzb,
                       const std::vector<double> &dxc, const std::vector<double> &dyc, const std::vector<double> &dzc,
                       double mu0, Recip *rc)
@@ -111,7 +114,7 @@ inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> 
         if (d.size() < to || from >= to) return false;
         const double x = d[from];
         int e;
-        if (!(x > 0.0) || !(x < DBL_MAX) || std::frexp(x, &e) != 0.5) return false;
+        if (!(x >= 0x1p-340) || !(x <= 0x1p340) || std::frexp(x, &e) != 0.5) return false;
         for (size_t q = from; q < to; ++q)
             if (d[q] != x) return false;
         *v = x;
@@ -119,7 +122,7 @@ inline bool pow2_grid(const std::vector<double> &dxb, const std::vector<double> 
     };
     double xb, yb, zb, xc, yc, zc;
     int e;
-    if (!(mu0 > 0.0) || !(mu0 < DBL_MAX) || std::frexp(mu0, &e) != 0.5) return false;
+    if (!(mu0 >= 0x1p-340) || !(mu0 <= 0x1p340) || std::frexp(mu0, &e) != 0.5) return false;
     // b: array indices 0 .. n+4 (i = -2 .. n+2); c: 1 .. n+4 (i = -1 .. n+2)
     if (!uniform(dxb, 0, dxb.size() - 1, &xb) || !uniform(dyb, 0, dyb.size() - 1, &yb) ||
         !uniform(dzb, 0, dzb.size() - 1, &zb) || !uniform(dxc, 1, dxc.size() - 1, &xc) ||

@@ -3,9 +3,8 @@
 //
 // Some hosts of this code cannot call cudaMalloc once they are running: a
 // Fortran or C simulation whose device memory all comes from its own pool
-// allocator, an application that has handed the rest of the GPU's memory to
-// other work and must not grow, or a loop that is being recorded into a CUDA
-// graph where allocation calls are not allowed.  sams_lare_step_noalloc lets
+// allocator, or an application that has handed the rest of the GPU's memory
+// to other work and must not grow its footprint.  sams_lare_step_noalloc lets
 // them advance a solve held in their own device buffers: they pass the 13
 // field arrays (inputs and outputs), and the step's scratch comes from one
 // fixed array compiled into this library.
@@ -88,6 +87,9 @@ extern "C" int sams_lare_step_noalloc(const sams_lare_params *params, const sams
     const sams_lare_params &p = *params;
     if (p.nx < 1 || p.ny < 1 || p.nz < 1 || !(p.x_max > p.x_min) || !(p.y_max > p.y_min) || !(p.z_max > p.z_min))
         return fail(SAMS_ERR_INVALID, "sams_lare_step_noalloc: empty grid or domain");
+    // per-dimension bound first, so that the box products below cannot overflow
+    if (p.nx > 60000 || p.ny > 60000 || p.nz > 60000)
+        return fail(SAMS_ERR_INVALID, "sams_lare_step_noalloc: grid too large (a dimension above 60000 cells)");
 
     // Fields are dense box buffers: -2..n+2 per dimension, z fastest.
     sams::Geom g{};

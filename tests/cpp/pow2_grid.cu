@@ -68,6 +68,20 @@ int main()
                 if (x / d[q] != x * rr[q]) ++bad;
             }
     }
+    // subnormal and tiny spacings are powers of two for frexp, but their
+    // reciprocals (or those of their products) overflow: rejected
+    for (double tiny : {0x1p-1060, 0x1p-400, 0x1p400}) {
+        std::vector<double> db(10, tiny), dc(10, tiny), ok(10, 0.5);
+        sams::Recip r{};
+        if (sams::pow2_grid(db, ok, ok, dc, ok, ok, 1.0, &r)) {
+            std::printf("spacing %a accepted\n", tiny);
+            ++bad;
+        }
+        if (sams::pow2_grid(ok, ok, ok, ok, ok, ok, tiny, &r)) {
+            std::printf("mu0 %a accepted\n", tiny);
+            ++bad;
+        }
+    }
     std::printf("{\"bad\": %d}\n", bad);
     return bad ? 1 : 0;
 }

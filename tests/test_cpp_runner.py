@@ -50,8 +50,13 @@ def test_runner_gpu_matches_oracle(runner_bin, nsteps, shape):
     assert '"mismatches": 0' in out and '"time_ok": true' in out, out
 
 
-# the reference tree, read in place (the same default as oracle/Makefile's REF)
-REF_OT = os.path.join(os.environ.get("SAMS_REFERENCE_TREE", "/root/reference"), "src", "InitialConditions", "OrszagTang")
+# the reference tree, read in place where oracle/Makefile found it
+def _ref_tree():
+    from oracle import lare_oracle as lo
+    return lo.reference_tree() or ""
+
+
+REF_OT = os.path.join(_ref_tree(), "src", "InitialConditions", "OrszagTang")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_OT), reason="reference tree not present on this machine")

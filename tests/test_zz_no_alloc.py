@@ -33,8 +33,13 @@ def _noalloc_fn():
     return fn
 
 
+# The long-z grids run the kernels that need many z values on this entry
+# point's dense rows: nz = 31 and nz = 290 run the out-of-place x / y sweep
+# (and its pointer swap on the caller's buffers), nz = 290 also the separate
+# z-sweep kernels used when a z line does not fit one block.
 @pytest.mark.parametrize("case,n,calls", [("ot", (24, 20, 8), (3, 2)), ("rf", (16, 14, 12), (2, 2)),
-                                          ("harris", (20, 12, 6), (2, 3)), ("ot", (16, 12, 2), (2, 2))])
+                                          ("harris", (20, 12, 6), (2, 3)), ("ot", (16, 12, 2), (2, 2)),
+                                          ("rf", (10, 8, 31), (2, 2)), ("ot", (6, 5, 290), (2, 1))])
 def test_noalloc_matches_regular_entry_point(case, n, calls):
     import torch
 
