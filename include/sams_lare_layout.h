@@ -76,16 +76,21 @@ static inline int64_t sams_box_index(int64_t ny, int64_t nz,
     return ((i + 2) * (ny + 5) + (j + 2)) * (nz + 5) + (k + 2);
 }
 
-/* Boundary-condition kinds a (field, dim, edge) slot can hold.  These are
- * the built-in SAMS boundary conditions
+/* Boundary-condition kinds a (field, dim, edge) slot can hold.  Kinds 1-4
+ * are the built-in SAMS boundary conditions
  * (include/boundaryConditions/builtInBoundaryConditions.h): simpleClamp :55,
- * simpleMirrorBC :145, simpleZeroGradientBC :224, simplePeriodicBC :252. */
+ * simpleMirrorBC :145, simpleZeroGradientBC :224, simplePeriodicBC :252.
+ * SAMS_BC_LARE_OTHER is the LARE "BC_OTHER" condition of the
+ * LARE3DInitialConditions package for that field, dimension and edge
+ * (src/InitialConditions/LARE/boundary.cpp; the plane copies and zeroed
+ * wall planes of sams_lare_bc_other.h); its value is unused. */
 enum sams_lare_bc_kind {
     SAMS_BC_NONE = 0,
     SAMS_BC_PERIODIC = 1,
     SAMS_BC_ZERO_GRADIENT = 2,
     SAMS_BC_MIRROR = 3,
-    SAMS_BC_CLAMP = 4
+    SAMS_BC_CLAMP = 4,
+    SAMS_BC_LARE_OTHER = 5
 };
 
 /* Simulation parameters of one LARE3D solve: the members of

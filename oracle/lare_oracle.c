@@ -18,6 +18,7 @@
  * is not repeated.
  */
 #include "lare_oracle.h"
+#include "sams_lare_bc_other.h"
 
 #include <float.h>
 #include <math.h>
@@ -103,6 +104,24 @@ static void bc_apply_edge(lo_state *s, int f, int d, int e)
     for (int q = 0; q < 3; ++q) {
         lo[q] = sams_lare_field_lb(f, q);
         hi[q] = n[q] + 2;
+    }
+    if (kind == SAMS_BC_LARE_OTHER) {
+        /* LARE BC_OTHER (src/InitialConditions/LARE/boundary.cpp): whole-plane
+         * copies or zeroed planes, one pw::assign after another */
+        int32_t dst[3], src[3];
+        const int np = sams_lare_other_planes(f, d, e, n[d], dst, src);
+        for (int q = 0; q < np; ++q) {
+            int64_t a[3] = {lo[0], lo[1], lo[2]}, b[3] = {hi[0], hi[1], hi[2]};
+            a[d] = b[d] = dst[q];
+            for (int64_t i = a[0]; i <= b[0]; ++i)
+                for (int64_t j = a[1]; j <= b[1]; ++j)
+                    for (int64_t k = a[2]; k <= b[2]; ++k) {
+                        int64_t p3[3] = {i, j, k};
+                        p3[d] = src[q];
+                        A[I3(i, j, k)] = src[q] == SAMS_PLANE_ZERO ? 0.0 : A[I3(p3[0], p3[1], p3[2])];
+                    }
+        }
+        return;
     }
     const int64_t dlb = st ? 0 : 1, dub = n[d];                 /* domain   */
     const int64_t glo = e == 0 ? lo[d] : (st ? n[d] : n[d] + 1); /* ghosts   */

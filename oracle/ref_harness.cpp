@@ -17,6 +17,7 @@
  *   lare_ref --case ot|rf|harris --nx N --ny N --nz N --steps S
  *            [--seed S] [--b0 B] [--ic FILE] [--dump FILE]
  *            [--dump-step S --dump-phase start|half|end] [--quiet]
+ *            [--rke] [--geometry G] [--domain x0 x1 y0 y1 z0 z1] [--lare-bcs]
  * Prints one JSON line with timing of the step loop.
  */
 #include "shared_data.h"
@@ -24,6 +25,10 @@
 #include "builtInBoundaryConditions.h"
 
 #include "sams_lare_ic.h"
+// the reference's own LARE-compatible IC package: its BC_OTHER boundary
+// functions (src/InitialConditions/LARE/boundary.cpp, compiled from the
+// reference tree) and their registration (lareic.h:96-140)
+#include "lareic.h"
 
 #include <chrono>
 #include <cstdio>
@@ -51,6 +56,7 @@ namespace oracle
         std::vector<double> dts, times, step_seconds;
         std::chrono::steady_clock::time_point last_mark;
         bool dumped = false;
+        bool lare_bcs = false;  // BC_OTHER on every edge, from the reference's LARE IC package
     };
     config g;
 
@@ -263,9 +269,19 @@ namespace oracle
             (void)data;
         }
 
-        void setBoundaryConditions(SAMS::harness &harness)
+        void setBoundaryConditions(SAMS::harness &harness, LARE::simulationData &data, SAMS::timeState &time)
         {
             using namespace SAMS;
+            if (g.lare_bcs)
+            {
+                // every edge BC_OTHER, registered by the reference package itself
+                data.xbc_min = data.xbc_max = LARE::BCType::BC_OTHER;
+                data.ybc_min = data.ybc_max = LARE::BCType::BC_OTHER;
+                data.zbc_min = data.zbc_max = LARE::BCType::BC_OTHER;
+                LARE::LARE3DInitialConditions lareIC;
+                lareIC.setBoundaryConditions(harness, data, time);
+                return;
+            }
             for (int f = 0; f < SAMS_NFIELDS; ++f)
             {
                 variableDef &vd = harness.variableRegistry.getVariable(sams_lare_field_names[f]);
@@ -353,6 +369,7 @@ int main(int argc, char *argv[])
         }
         else if (a == "--quiet") quiet = true;
         else if (a == "--rke") rke = true;
+        else if (a == "--lare-bcs") g.lare_bcs = true;
         else if (a == "--geometry") geometry = std::atoi(arg_value(i, argc, argv));
         else if (a == "--domain")
         {

@@ -253,7 +253,7 @@ __global__ void kb_bc_edge(const Ctx *__restrict__ ctxs, const BcTable *__restri
             q[0] = sl.lo[0] + (int)(t / ((long long)e1 * e2));
             q[1] = sl.lo[1] + (int)((t / e2) % e1);
             q[2] = sl.lo[2] + (int)(t % e2);
-            bc_edge_apply(c.f[f], g, sl, kind, bt.value[f][d][e], d, e, q);
+            bc_edge_apply(c.f[f], g, sl, bt, f, d, e, q);
         }
     }
 }
@@ -373,16 +373,14 @@ int Batch::add(const sams_lare_params &p, const sams_lare_bcs &bcs, int *id)
     if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
     BatchSlot s;
     s.p = p;
+    {
+        const long long n[3] = {p.nx, p.ny, p.nz};
+        if (!bc_table_from(s.bc, bcs, n, &err)) return SAMS_ERR_INVALID;
+    }
     for (int f = 0; f < SAMS_NFIELDS; ++f) {
         bool per = true;
         for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 2; ++e) {
-                int k = bcs.kind[f][d][e];
-                if (k < SAMS_BC_NONE || k > SAMS_BC_CLAMP) { err = "unknown boundary-condition kind"; return SAMS_ERR_INVALID; }
-                s.bc.kind[f][d][e] = (signed char)k;
-                s.bc.value[f][d][e] = bcs.value[f][d][e];
-                per = per && k == SAMS_BC_PERIODIC;
-            }
+            for (int e = 0; e < 2; ++e) per = per && bcs.kind[f][d][e] == SAMS_BC_PERIODIC;
         // the one-pass periodic gather needs every source inside the domain
         if (per && std::min(p.nx, std::min(p.ny, p.nz)) >= kBcSequentialBelow) s.periodic_groups |= 1u << f;
     }

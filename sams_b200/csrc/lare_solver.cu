@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(kThreads) k_bc_edge(Ctx c, FieldList fl, BcTab
     q[0] = sl.lo[0] + (int)(t / ((long long)e1 * e2));
     q[1] = sl.lo[1] + (int)((t / e2) % e1);
     q[2] = sl.lo[2] + (int)(t % e2);
-    bc_edge_apply(c.f[f], g, sl, kind, bt.value[f][d][e], d, e, q);
+    bc_edge_apply(c.f[f], g, sl, bt, f, d, e, q);
 }
 
 FieldList make_list(unsigned mask)
@@ -370,14 +370,10 @@ int Solver::init_impl(const sams_lare_params &p, const sams_lare_bcs &bcs, int d
     }
     p_ = p;
     device_ = device;
-    for (int f = 0; f < SAMS_NFIELDS; ++f)
-        for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 2; ++e) {
-                int k = bcs.kind[f][d][e];
-                if (k < SAMS_BC_NONE || k > SAMS_BC_CLAMP) { err = "unknown boundary-condition kind"; return SAMS_ERR_INVALID; }
-                bc_.kind[f][d][e] = (signed char)k;
-                bc_.value[f][d][e] = bcs.value[f][d][e];
-            }
+    {
+        const long long n[3] = {p.nx, p.ny, p.nz};
+        if (!bc_table_from(bc_, bcs, n, &err)) return SAMS_ERR_INVALID;
+    }
     int rc;
     if ((rc = check(cudaSetDevice(device), "cudaSetDevice"))) return rc;
     if ((rc = check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "sm count")))
@@ -476,17 +472,16 @@ int Solver::init_borrowed(const sams_lare_params &p, const sams_lare_bcs &bcs, c
     }
     p_ = p;
     device_ = device;
-    for (int f = 0; f < SAMS_NFIELDS; ++f)
-        for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 2; ++e) {
-                int k = bcs.kind[f][d][e];
-                if (k < SAMS_BC_NONE || k > SAMS_BC_CLAMP) { err = "unknown boundary-condition kind"; return SAMS_ERR_INVALID; }
-                bc_.kind[f][d][e] = (signed char)k;
-                bc_.value[f][d][e] = bcs.value[f][d][e];
-            }
+    {
+        const long long n[3] = {p.nx, p.ny, p.nz};
+        if (!bc_table_from(bc_, bcs, n, &err)) return SAMS_ERR_INVALID;
+    }
     ctx_ = ctx;
     sc_ = ctx.sc;  // borrowed: release_borrowed() must clear it before destruction
     stream_ = stream;
+    int rc;
+    if ((rc = check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "sm count")))
+        return rc;
     return setup_psweep();
 }
 
@@ -499,13 +494,14 @@ void Solver::release_borrowed()
 
 int Solver::set_bc(int field, int dim, int edge, int kind, double value)
 {
-    if (field < 0 || field >= SAMS_NFIELDS || dim < 0 || dim > 2 || edge < 0 || edge > 1 || kind < SAMS_BC_NONE ||
-        kind > SAMS_BC_CLAMP) {
+    if (field < 0 || field >= SAMS_NFIELDS || dim < 0 || dim > 2 || edge < 0 || edge > 1) {
         err = "invalid boundary-condition slot or kind";
         return SAMS_ERR_INVALID;
     }
-    bc_.kind[field][dim][edge] = (signed char)kind;
-    bc_.value[field][dim][edge] = value;
+    const long long n[3] = {p_.nx, p_.ny, p_.nz};
+    BcTable t = bc_;
+    if (!bc_slot_set(t, field, dim, edge, kind, value, n, &err)) return SAMS_ERR_INVALID;
+    bc_ = t;
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     graphs_.clear();
     return SAMS_OK;

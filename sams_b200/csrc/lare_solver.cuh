@@ -8,15 +8,10 @@
 #include <vector>
 
 #include "lare_device.cuh"
+#include "lare_bc.cuh"
 #include "sams_lare.h"
 
 namespace sams {
-
-// Boundary conditions of all fields as the kernels read them.
-struct BcTable {
-    signed char kind[SAMS_NFIELDS][3][2];
-    double value[SAMS_NFIELDS][3][2];
-};
 
 // Sets of fields filled together (the LARE3D *_bcs groups,
 // src/PhysicsPackages/LARE/boundary.cpp:27-97).

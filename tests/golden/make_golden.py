@@ -52,6 +52,15 @@ CASES = [
     ("ot_p2_16x8x4_s4", "ot", 16, 8, 4, 4, 1, 0.0),
     ("rf_p2_rke_16x8x8_s4", "rf", 16, 8, 8, 4, 7, 0.0, {"rke": 1}),
     ("harris_p2_16x8x4_s3", "harris", 16, 8, 4, 3, 3, 0.0, {"domain": [-8.0, 8.0, -4.0, 4.0, 0.0, 2.0]}),
+    # the LARE BC_OTHER conditions of the reference's LARE3DInitialConditions
+    # package on every edge (walls in x for the velocities, plane copies
+    # elsewhere), registered by that package itself in the reference run
+    ("ot_lare_12x10x6_s5", "ot", 12, 10, 6, 5, 1, 0.0, {"lare_bcs": 1}),
+    ("rf_lare_10x8x6_s4", "rf", 10, 8, 6, 4, 7, 0.0, {"lare_bcs": 1}),
+    ("ot_lare_8x6x2_s3", "ot", 8, 6, 2, 3, 1, 0.0, {"lare_bcs": 1}),
+    ("harris_lare_p2_16x8x4_s3", "harris", 16, 8, 4, 3, 3, 0.0,
+     {"lare_bcs": 1, "domain": [-8.0, 8.0, -4.0, 4.0, 0.0, 2.0]}),
+    ("ot_lare_rke_12x10x6_s4", "ot", 12, 10, 6, 4, 1, 0.0, {"lare_bcs": 1, "rke": 1}),
 ]
 STATE = ["rho", "energy_electron", "energy_ion", "vx", "vy", "vz", "bx", "by", "bz"]
 # (file, case, nx, ny, nz, steps, seed): the reference's full harness state
@@ -71,7 +80,9 @@ def main(only=()):
             continue
         o = opt[0] if opt else {}
         rke, geometry, domain = o.get("rke", 0), o.get("geometry", 0), o.get("domain")
+        lare_bcs = o.get("lare_bcs", 0)
         extra = (["--rke"] if rke else []) + (["--geometry", str(geometry)] if geometry else [])
+        extra += ["--lare-bcs"] if lare_bcs else []
         if domain:
             extra += ["--domain"] + [repr(x) for x in domain]
         with tempfile.TemporaryDirectory() as td:
@@ -84,7 +95,7 @@ def main(only=()):
                 out[f] = d.box(f)
             out["dts"] = np.array(d.header["dts"])
             meta = dict(case=case, nx=nx, ny=ny, nz=nz, steps=steps, seed=seed, b0=b0, rke=rke, geometry=geometry,
-                        domain=domain,
+                        domain=domain, lare_bcs=lare_bcs,
                         time=summary["time"], generator="oracle/_ref/lare_ref (reference LARE3D)")
             out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -112,12 +123,22 @@ if __name__ == "__main__":
     main(tuple(sys.argv[1:]))
 
 
-def apply_options(p, meta):
+SAMS_BC_LARE_OTHER = 5  # include/sams_lare_layout.h
+
+
+def apply_options(p, meta, b=None):
     """Set a case's rke / geometry / domain options (from a fixture's meta) on
-    a parameter block of either ctypes binding."""
+    a parameter block of either ctypes binding, and, given its boundary
+    conditions `b`, the LARE BC_OTHER condition on every edge of every field
+    where the case asks for it (lare_bcs)."""
     p.rke = meta.get("rke", 0)
     p.geometry = meta.get("geometry", 0)
     d = meta.get("domain")
     if d:
         p.x_min, p.x_max, p.y_min, p.y_max, p.z_min, p.z_max = d
+    if b is not None and meta.get("lare_bcs"):
+        for f in range(len(b.kind)):
+            for dim in range(3):
+                for e in range(2):
+                    b.kind[f][dim][e] = SAMS_BC_LARE_OTHER
     return p

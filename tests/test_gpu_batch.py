@@ -110,3 +110,29 @@ def test_batch_mixing_geometries_equals_solo():
         ref, st = _solo(case, n, seed, b0, 4, rke, geo)
         _check_equal(bt, sid, case, n, ref, st)
     bt.close()
+
+
+def test_batch_with_lare_other_bcs_equals_solo():
+    """Solves whose every edge carries the LARE BC_OTHER conditions, batched
+    with periodic ones: each equals its solo run."""
+    mix = [("ot", (16, 12, 4), 1, 0.0, True), ("rf", (12, 12, 12), 3, 0.0, True),
+           ("ot", (20, 16, 2), 6, 0.0, True), ("ot", (24, 24, 4), 2, 0.0, False)]
+    steps = 5
+    bt = lare.Batch()
+    ids, refs = [], []
+    for case, n, seed, b0, lbc in mix:
+        opts = {"lare_bcs": 1} if lbc else {}
+        p, b = lare.case_setup(case, *n, b0)
+        apply_options(p, opts, b)
+        ids.append(bt.add(p, b, lare.case_fields(case, p, seed=seed, b0=b0)))
+        s = lare.LARE3D(p, b)
+        s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
+        s.step(steps)
+        refs.append(({f: s.download(f) for f in STATE}, (s.dt, s.time, s.steps)))
+        s.close()
+    bt.step(steps, graph=True)
+    bt.synchronize()
+    for sid, (case, n, seed, b0, lbc), (ref, st) in zip(ids, mix, refs):
+        _check_equal(bt, sid, case, n, ref, st)
+    bt.close()
+

@@ -18,7 +18,7 @@ def _solver(case, nx, ny, nz, seed=1, b0=0.0, rke=0, options=None):
     p, b = lare.case_setup(case, nx, ny, nz, b0)
     p.rke = rke
     if options:
-        apply_options(p, options)
+        apply_options(p, options, b)
     s = lare.LARE3D(p, b)
     s.upload_all(lare.case_fields(case, p, seed=seed, b0=b0))
     return s
@@ -190,3 +190,29 @@ def test_gpu_matches_checker_in_curvilinear_geometry(case, n, steps, geometry, r
         o.step(1)
         assert s.dt == o.dt
     _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"geometry {geometry} {case}{n}")
+
+
+# The LARE BC_OTHER conditions (walls at the x edges for the velocities,
+# plane copies elsewhere) on every edge, as the reference's
+# LARE3DInitialConditions package installs them, against the C restatement
+# (itself pinned to the reference's own run of that package by the
+# *_lare_* fixtures): sizes with fused x / y sweeps (nz >= 24), 2.5-D and a
+# power-of-two grid.
+@pytest.mark.parametrize("case,n,steps", [
+    ("ot", (20, 16, 8), 8), ("rf", (12, 10, 26), 4), ("harris", (10, 12, 28), 3),
+    ("ot", (16, 12, 2), 4), ("rf", (16, 16, 16), 4),
+])
+def test_gpu_lare_other_bcs_match_checker(case, n, steps, oracle_lib):
+    lo = oracle_lib
+    nx, ny, nz = n
+    opts = {"lare_bcs": 1}
+    s = _solver(case, nx, ny, nz, seed=5, options=opts)
+    p, b = lo.case_setup(case, nx, ny, nz)
+    apply_options(p, opts, b)
+    o = lo.Oracle(p, b, lo.case_fields(case, p, seed=5))
+    for _ in range(steps):
+        s.step(1)
+        o.step(1)
+        assert s.dt == o.dt
+    _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"lare bcs {case}{n}")
+    s.close()

@@ -16,7 +16,7 @@ from tests.golden.make_golden import CASES, GEO_DOMAIN, STATE, apply_options, lo
 
 def _run_checker(case, nx, ny, nz, steps, seed, b0, options=None):
     p, b = lo.case_setup(case, nx, ny, nz, b0)
-    apply_options(p, options or {})
+    apply_options(p, options or {}, b)
     o = lo.Oracle(p, b, lo.case_fields(case, p, seed=seed, b0=b0))
     dts = []
     for _ in range(steps):
