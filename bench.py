@@ -158,18 +158,38 @@ def ncu_traffic(n):
         return None
 
 
+def fp64_roof(n, ms_per_step, rates):
+    """The step's FP64 compute roof: its fp64-pipe warp instructions (ncu
+    sm__inst_executed_pipe_fp64 over one step of this workload, committed in
+    profiles/lare_step_rf{n}_fp64.json) at the measured fused multiply-add
+    rate (one warp instruction = 32 thread operations), against the step's
+    measured time."""
+    path = os.path.join(ROOT, "profiles", f"lare_step_rf{n}_fp64.json")
+    try:
+        with open(path) as f:
+            inst = float(json.load(f)["fp64_pipe_warp_inst_per_step"])
+    except Exception:
+        return None
+    if not rates or not rates.get("fma"):
+        return None
+    roof_ms = inst * 32 / (rates["fma"] * 1e9) * 1e3
+    return {"fp64_pipe_warp_inst_per_step": inst, "roof_ms": roof_ms, "frac": roof_ms / ms_per_step,
+            "source": os.path.relpath(path, ROOT)}
+
+
 def cpu_reference(n, steps, threads=None):
     """Time the reference LARE3D CPU code (or, without its binary, the C
     restatement) on this host for `steps` steps of the n^3 workload."""
     from oracle import lare_oracle as lo
     threads = threads or os.cpu_count()
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
-    if os.path.exists(lo.REF_BENCH_BIN):
-        cmd = [lo.REF_BENCH_BIN, "--case", "rf", "--nx", str(n), "--ny", str(n), "--nz", str(n),
+    binary, isa = lo.reference_bench_binary()
+    if os.path.exists(binary):
+        cmd = [binary, "--case", "rf", "--nx", str(n), "--ny", str(n), "--nz", str(n),
                "--steps", str(steps), "--seed", "1", "--quiet"]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
         rec = json.loads(out.strip().splitlines()[-1])
-        return rec["step_seconds"], "reference", threads
+        return rec["step_seconds"], "reference", threads, isa
     # the C restatement (ctypes, OpenMP)
     p, b = lo.case_setup("rf", n, n, n)
     o = lo.Oracle(p, b, lo.case_fields("rf", p, seed=1))
@@ -178,7 +198,7 @@ def cpu_reference(n, steps, threads=None):
         t0 = time.perf_counter()
         o.step(1)
         secs.append(time.perf_counter() - t0)
-    return secs, "port", threads
+    return secs, "port", threads, "-O2 C restatement"
 
 
 def max_over_ranks(pg, ms, device):
@@ -203,7 +223,7 @@ def run_reference_arm(args, world, rank):
         return
     n = args.edge
     total = args.warmup + args.steps
-    secs, kind, threads = cpu_reference(n, total)
+    secs, kind, threads, isa = cpu_reference(n, total)
     timed = secs[args.warmup:]
     cells = float(n) ** 3
     value = cells * len(timed) / sum(timed)
@@ -213,7 +233,7 @@ def run_reference_arm(args, world, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": workload(n), "case": "rf", "grid": [n, n, n], "parallelism": "cpu-openmp"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "isa": isa,
                          "sample": f"{len(timed)} timed steps of the {n}^3 workload after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -262,6 +282,8 @@ def run_sams(args, world, rank, local, pg):
     phases = s.phase_times()
     s.synchronize()
     s.close()
+    # the compute roof's denominators: measured FP64 rates of this GPU
+    fp64 = {k: v / 1e9 for k, v in lare.fp64_rates(local).items()} if rank == 0 else None
 
     # ---------------- end to end through the C ABI ----------------
     e2e = None
@@ -320,9 +342,9 @@ def run_sams(args, world, rank, local, pg):
     if world == 1 and not args.no_cpu_baseline:
         try:
             csteps = 4 if n >= 256 else 8
-            secs, kind, threads = cpu_reference(n, csteps)
+            secs, kind, threads, isa = cpu_reference(n, csteps)
             cpu = {"value": cells * len(secs) / sum(secs), "unit": UNIT, "cores": threads, "kind": kind,
-                   "sample": f"{csteps} steps of the {n}^3 workload (all steps timed)"}
+                   "isa": isa, "sample": f"{csteps} steps of the {n}^3 workload (all steps timed)"}
         except Exception as ex:  # report, do not fail the GPU line
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
@@ -338,6 +360,8 @@ def run_sams(args, world, rank, local, pg):
         "batched": batched,
         "served": served,
         "phases_ms": dict(zip(["lagrangian", "corrector", "remap_x", "remap_y", "remap_z"], phases)),
+        "fp64_rates_gops": fp64,
+        "fp64_roof": fp64_roof(n, ms_per_step, fp64),
     }
     print(json.dumps(line), flush=True)
 

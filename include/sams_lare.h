@@ -131,6 +131,14 @@ int sams_lare_phase_times(sams_lare_solver *h, double ms[5]);
 /* Number of kernel launches one sams_lare_step(h, 1) issues. */
 int sams_lare_launches_per_step(sams_lare_solver *h, int64_t *launches);
 
+/* No counterpart in the reference (it has no performance model).  Measured
+ * FP64 throughput of `device`, in thread-level operations per second, for
+ * the compute roof of the step: rates[0] add, [1] multiply, [2] fused
+ * multiply-add, [3] IEEE division by data, [4] IEEE square root (with one
+ * multiply), [5] correctly rounded reciprocal (with one multiply).  Runs
+ * for about a second on an idle B200. */
+int sams_lare_fp64_rates(int device, double rates[6]);
+
 /* ---- Batched solves ----------------------------------------------------
  * Many independent LARE3D solves (any mix of sizes, parameters and boundary
  * conditions) stepped together: each phase of the step is one persistent

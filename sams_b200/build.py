@@ -16,7 +16,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libsams_lare.so")
 
 CU_SOURCES = ["lare_solver.cu", "lare_batch.cu", "lare_serve.cu", "lare_capi.cu", "lare_noalloc.cu", "lare_dump.cu",
-              "lare_router.cu", "lare_dist.cu"]
+              "lare_router.cu", "lare_dist.cu", "lare_fp64_roof.cu"]
 C_SOURCES = ["lare_ic.c"]
 HEADERS = ["lare_device.cuh", "lare_ops.cuh", "lare_solver.cuh", "lare_batch.cuh"]
 

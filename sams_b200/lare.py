@@ -92,6 +92,7 @@ def lib():
     L.sams_lare_device_bytes.argtypes = [vp, ctypes.POINTER(i64)]
     L.sams_lare_launches_per_step.argtypes = [vp, ctypes.POINTER(i64)]
     L.sams_lare_phase_times.argtypes = [vp, _P]
+    L.sams_lare_fp64_rates.argtypes = [ctypes.c_int, _P]
     L.sams_lare_save.argtypes = [vp, ctypes.c_char_p]
     L.sams_lare_load.argtypes = [vp, ctypes.c_char_p]
     L.sams_lare_case_setup.argtypes = [ctypes.c_int, i64, i64, i64, ctypes.c_double,
@@ -109,6 +110,18 @@ def _check(rc):
 
 def box_shape(nx, ny, nz):
     return (nx + 5, ny + 5, nz + 5)
+
+
+FP64_KINDS = ("add", "mul", "fma", "div", "sqrt", "rcp")
+
+
+def fp64_rates(device=0):
+    """Measured FP64 throughput of `device` (thread-level operations per
+    second) by kind: add, mul, fma, IEEE div, sqrt (with one multiply),
+    correctly rounded reciprocal (with one multiply)."""
+    out = (ctypes.c_double * 6)()
+    _check(lib().sams_lare_fp64_rates(device, out))
+    return dict(zip(FP64_KINDS, list(out)))
 
 
 def field_slices(field, nx, ny, nz):
