@@ -24,12 +24,15 @@
 #pragma once
 
 #include <cstring>
+#include <map>
+#include <vector>
 #include <limits>
 #include <stdexcept>
 #include <string>
 #include <string_view>
 
 #include "sams_runner.hpp"
+#include "../sams_lare_bc_other.h"
 
 namespace LARE {
 
@@ -39,8 +42,14 @@ using SAMS::T_indexType;
 
 enum class geometryType { Cartesian = 0, Cylindrical = 1, Spherical = 2 };
 
+// LARE-style boundary types (shared_data.h:46-54); BC_OTHER edges get the
+// IC package's own boundary functions, BC_EXTERNAL edges none.
+enum class BCType { BC_OTHER = 0, BC_PERIODIC = 1, BC_REFLECTIVE = 2, BC_OUTFLOW = 3, BC_INFLOW = 4, BC_EXTERNAL = 5 };
+
 // The members of the reference simulationData that initial-condition
-// packages set or read (shared_data.h:60-131).
+// packages set or read (shared_data.h:60-226), including host views of the
+// 13 harness variables (bound in getVariables, as LARE3D::getVariables binds
+// them, setup.cpp:95-140).
 struct simulationData {
     T_dataType dt = 0.0, dtr = 0.0, dt_multiplier = 0.8;
     T_dataType time = 0.0;
@@ -60,6 +69,21 @@ struct simulationData {
     T_dataType mf = 1.2;
     T_dataType mu0 = 4.0e-7 * 3.14159265358979323846;
     T_dataType dt_snapshots = 0.0;
+    T_dataType lastOutputTime = 0.0;
+    BCType xbc_min = BCType::BC_OTHER, xbc_max = BCType::BC_OTHER;
+    BCType ybc_min = BCType::BC_OTHER, ybc_max = BCType::BC_OTHER;
+    BCType zbc_min = BCType::BC_OTHER, zbc_max = BCType::BC_OTHER;
+    bool x_stretch = false, y_stretch = false, z_stretch = false;
+    // one process holds the whole domain, so it is on every edge
+    bool isxLB = true, isxUB = true, isyLB = true, isyUB = true, iszLB = true, iszUB = true;
+    using volumeArray = pw::portableArray<T_dataType, 3>;
+    volumeArray rho, energy_electron, energy_ion, vx, vy, vz, vx1, vy1, vz1, bx, by, bz, dm;
+    volumeArray *field(int f)
+    {
+        volumeArray *a[SAMS_NFIELDS] = {&rho, &energy_electron, &energy_ion, &vx, &vy, &vz, &vx1,
+                                        &vy1, &vz1, &bx, &by, &bz, &dm};
+        return a[f];
+    }
 };
 
 // The remap's working arrays live in the solver's device scratch.
@@ -111,6 +135,17 @@ public:
         d.rke = false;
         d.mu0 = 4.0e-7 * 3.14159265358979323846;
         d.time = 0.0;
+    }
+
+    // Host views of the harness variables (LARE3D::getVariables,
+    // setup.cpp:95-140).
+    void getVariables(SAMS::harness &h, simulationData &d)
+    {
+        for (int f = 0; f < SAMS_NFIELDS; ++f) h.variableRegistry.fillPPArray(sams_lare_field_names[f], *d.field(f));
+        const auto &X = h.axisRegistry.get("X"), &Y = h.axisRegistry.get("Y"), &Z = h.axisRegistry.get("Z");
+        d.nx = X.n;
+        d.ny = Y.n;
+        d.nz = Z.n;
     }
 
     void defaultVariables(simulationData &)
@@ -180,7 +215,8 @@ public:
 
     // The boundary-condition table built from what the IC package attached
     // to each harness variable (one condition per variable, dimension and
-    // edge; the built-in conditions only).
+    // edge): the built-in conditions by kind; a condition defined only by
+    // its host apply() (LAREBoundaryConditions) by probing it.
     static sams_lare_bcs bcs(SAMS::harness &h)
     {
         sams_lare_bcs b;
@@ -194,11 +230,76 @@ public:
                     if (list.size() > 1)
                         throw std::runtime_error("LARE3D: variable " + v.name +
                                                  " has more than one boundary condition on one edge");
-                    b.kind[v.field][d][e] = list.front()->kind();
+                    int kind = list.front()->kind();
+                    if (kind == SAMS::boundaryConditions::kHostDefined) kind = probe(h, v, *list.front(), d, e);
+                    b.kind[v.field][d][e] = kind;
                     b.value[v.field][d][e] = list.front()->value();
                 }
         }
         return b;
+    }
+
+    // Run a host-defined condition's apply(d, e) once on the variable's box
+    // filled with distinct tags (restored afterwards) and read off what it
+    // did: which ghost planes of dimension d received a copy of which plane,
+    // or zero.  The result must be exactly the LARE BC_OTHER table of that
+    // variable (sams_lare_bc_other.h: what the reference's
+    // LARE3DInitialConditions functions do), or nothing at all; anything else
+    // has no device descriptor and is refused.
+    static int probe(SAMS::harness &h, const SAMS::variableDef &v, SAMS::boundaryConditions &bc, int d, int e)
+    {
+        const auto &X = h.axisRegistry.get("X"), &Y = h.axisRegistry.get("Y"), &Z = h.axisRegistry.get("Z");
+        const long long n[3] = {X.n, Y.n, Z.n};
+        const long long ext[3] = {n[0] + 5, n[1] + 5, n[2] + 5};
+        const int f = v.field;
+        double *box = h.variableRegistry.box(f);
+        const long long ne = ext[0] * ext[1] * ext[2];
+        const double base = 1048576.0;  // tags base + t are exact, distinct and nonzero
+        std::vector<double> keep(box, box + ne);
+        for (long long t = 0; t < ne; ++t) box[t] = base + (double)t;
+        bc.apply(d, e == 0 ? SAMS::domain::edges::lower : SAMS::domain::edges::upper);
+        // per destination plane: the source plane (or kZero), and how many points
+        const long long kZero = -1000000, kUnset = -2000000;
+        std::map<long long, std::pair<long long, long long>> planes;
+        bool ok = true;
+        for (long long t = 0; t < ne && ok; ++t) {
+            if (box[t] == base + (double)t) continue;
+            const long long q[3] = {t / (ext[1] * ext[2]) - 2, (t / ext[2]) % ext[1] - 2, t % ext[2] - 2};
+            long long src = kUnset;
+            if (box[t] == 0.0) {
+                src = kZero;
+            } else {
+                const double tv = box[t] - base;
+                const long long u = (long long)tv;
+                if (!(tv >= 0.0) || (double)u != tv || u >= ne) { ok = false; break; }
+                const long long r[3] = {u / (ext[1] * ext[2]) - 2, (u / ext[2]) % ext[1] - 2, u % ext[2] - 2};
+                for (int o = 0; o < 3; ++o)
+                    if (o != d && r[o] != q[o]) ok = false;
+                src = r[d];
+            }
+            auto it = planes.find(q[d]);
+            if (it == planes.end()) planes[q[d]] = {src, 1};
+            else if (it->second.first != src) ok = false;
+            else ++it->second.second;
+        }
+        std::copy(keep.begin(), keep.end(), box);
+        if (planes.empty() && ok) return SAMS_BC_NONE;
+        int32_t dst[3], srcs[3];
+        const int np = sams_lare_other_planes(f, d, e, n[d], dst, srcs);
+        long long plane = 1;  // points of one plane of the variable's own range
+        for (int o = 0; o < 3; ++o)
+            if (o != d) plane *= n[o] + 3 - sams_lare_field_lb(f, o);
+        ok = ok && (int)planes.size() == np;
+        for (int q = 0; q < np && ok; ++q) {
+            auto it = planes.find(dst[q]);
+            const long long want = srcs[q] == SAMS_PLANE_ZERO ? kZero : srcs[q];
+            ok = it != planes.end() && it->second.first == want && it->second.second == plane;
+        }
+        if (!ok)
+            throw std::runtime_error("LARE3D: the boundary condition of " + v.name + " (dimension " +
+                                     std::to_string(d) + ", edge " + std::to_string(e) +
+                                     ") is neither a built-in condition nor the LARE BC_OTHER planes");
+        return SAMS_BC_LARE_OTHER;
     }
 
 private:

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdint>
 #include <functional>
+#include <iostream>
 #include <limits>
 #include <map>
 #include <memory>
@@ -45,15 +46,19 @@ namespace portableWrapper {
 
 struct Range {
     long long lower_bound, upper_bound;
+    bool all = false;  // Range(): every index of the dimension it slices
     Range(long long lb, long long ub) : lower_bound(lb), upper_bound(ub) {}
     explicit Range(long long n) : lower_bound(1), upper_bound(n) {}
-    Range() : lower_bound(0), upper_bound(-1) {}
+    Range() : lower_bound(0), upper_bound(-1), all(true) {}
 };
 
 enum class arrayTags { host = 0, accelerated = 1 };
 
 // A view over host memory with the reference's index ranges (any lower bound,
-// last index fastest).
+// last index fastest).  Indexing with all integers gives an element; with
+// some Range arguments it gives a view of lower rank over those dimensions
+// (the reference's slicing, e.g. a(-2, Range(), Range()) is the plane -2 of
+// dimension 0, include/pp/array.h).
 template <typename T, int N, arrayTags tag = arrayTags::accelerated>
 class portableArray {
 public:
@@ -68,13 +73,40 @@ public:
         }
     }
     template <typename... I>
-    T &operator()(I... idx) const
+    decltype(auto) operator()(I... idx) const
     {
         static_assert(sizeof...(I) == N, "wrong number of indices");
-        const long long ix[N] = {(long long)idx...};
-        long long o = 0;
-        for (int d = 0; d < N; ++d) o += (ix[d] - lb_[d]) * st_[d];
-        return data_[o];
+        if constexpr ((std::is_integral_v<I> && ...)) {
+            const long long ix[N] = {(long long)idx...};
+            long long o = 0;
+            for (int d = 0; d < N; ++d) o += (ix[d] - lb_[d]) * st_[d];
+            return static_cast<T &>(data_[o]);
+        } else {
+            constexpr int M = ((std::is_same_v<I, Range> ? 1 : 0) + ...);
+            static_assert(M > 0 && M <= N, "a slice keeps at least one dimension");
+            portableArray<T, M, tag> v;
+            long long lb[M], ub[M], st[M], off = 0;
+            int d = 0, m = 0;
+            auto one = [&](const auto &x) {
+                if constexpr (std::is_same_v<std::decay_t<decltype(x)>, Range>) {
+                    const long long a = x.all ? lb_[d] : x.lower_bound, b = x.all ? ub_[d] : x.upper_bound;
+                    if (a < lb_[d] || b > ub_[d]) throw std::out_of_range("portableArray: slice outside the array");
+                    lb[m] = a;
+                    ub[m] = b;
+                    st[m] = st_[d];
+                    off += (a - lb_[d]) * st_[d];
+                    ++m;
+                } else {
+                    if ((long long)x < lb_[d] || (long long)x > ub_[d])
+                        throw std::out_of_range("portableArray: index outside the array");
+                    off += ((long long)x - lb_[d]) * st_[d];
+                }
+                ++d;
+            };
+            (one(idx), ...);
+            v.bind(data_ + off, lb, ub, st);
+            return v;
+        }
     }
     Range getRange(int d) const { return Range(lb_[d], ub_[d]); }
     T *data() const { return data_; }
@@ -118,14 +150,55 @@ void applyKernel(F f, Range a, Range b, Range c)
 }
 inline void fence() {}
 
+namespace detail {
+// Visit every element of an N-d view (last index fastest): f(offset of dst)
+template <typename T, int N, arrayTags tag, typename F>
+void each_index(const portableArray<T, N, tag> &a, F f)
+{
+    long long ix[N];
+    for (int d = 0; d < N; ++d) {
+        ix[d] = a.getRange(d).lower_bound;
+        if (a.getRange(d).upper_bound < ix[d]) return;
+    }
+    for (;;) {
+        f(ix);
+        int d = N - 1;
+        while (d >= 0 && ++ix[d] > a.getRange(d).upper_bound) {
+            ix[d] = a.getRange(d).lower_bound;
+            --d;
+        }
+        if (d < 0) return;
+    }
+}
+template <typename T, int N, arrayTags tag>
+T &at(const portableArray<T, N, tag> &a, const long long *ix)
+{
+    if constexpr (N == 1) return a(ix[0]);
+    else if constexpr (N == 2) return a(ix[0], ix[1]);
+    else return a(ix[0], ix[1], ix[2]);
+}
+}  // namespace detail
+
+// pw::assign(array or slice, value) and pw::assign(array or slice, array or
+// slice of the same extents) (include/pp/algorithm.h): element by element,
+// the source indexed at the same offsets from its own lower bounds.
 template <typename T, int N, arrayTags tag, typename V>
 void assign(portableArray<T, N, tag> a, const V &v)
 {
-    if constexpr (N == 3)
-        applyKernel([&](long long i, long long j, long long k) { a(i, j, k) = v; }, a.getRange(0), a.getRange(1),
-                    a.getRange(2));
-    else
-        for (long long i = a.getRange(0).lower_bound; i <= a.getRange(0).upper_bound; ++i) a(i) = v;
+    if constexpr (std::is_same_v<V, portableArray<T, N, arrayTags::accelerated>> ||
+                  std::is_same_v<V, portableArray<T, N, arrayTags::host>>) {
+        for (int d = 0; d < N; ++d)
+            if (a.getRange(d).upper_bound - a.getRange(d).lower_bound !=
+                v.getRange(d).upper_bound - v.getRange(d).lower_bound)
+                throw std::runtime_error("Error: pw::assign between arrays of different extents");
+        detail::each_index(a, [&](const long long *ix) {
+            long long jx[N];
+            for (int d = 0; d < N; ++d) jx[d] = ix[d] - a.getRange(d).lower_bound + v.getRange(d).lower_bound;
+            detail::at(a, ix) = detail::at(v, jx);
+        });
+    } else {
+        detail::each_index(a, [&](const long long *ix) { detail::at(a, ix) = v; });
+    }
 }
 
 }  // namespace portableWrapper
@@ -133,6 +206,8 @@ void assign(portableArray<T, N, tag> a, const V &v)
 namespace SAMS {
 
 namespace pw = portableWrapper;
+// SAMS::cout (rank-0 output in the reference; one process here)
+inline std::ostream &cout = std::cout;
 using T_dataType = double;
 using T_indexType = long long;
 using T_sizeType = long long;
@@ -157,13 +232,20 @@ struct dimension {
 class variableDef;
 
 // Boundary-condition objects.  On the GPU path a condition is a descriptor
-// (kind, value) executed by the device fill kernels; there is no virtual
-// apply() on host data.
+// (kind, value) executed by the device fill kernels.  The built-in
+// conditions name their kind.  A condition that only implements apply(dim,
+// edge) on the host arrays (the reference's interface,
+// include/boundaryConditions/boundaryConditions.h:9-15, as the LARE IC
+// package's LAREBoundaryConditions does) reports kHostDefined; LARE::LARE3D
+// then runs its apply() once on tagged host data at set-up and translates
+// the plane copies it observes into a device descriptor (or refuses it).
 class boundaryConditions {
 public:
+    static constexpr int kHostDefined = -1;
     virtual ~boundaryConditions() = default;
-    virtual int kind() const = 0;
+    virtual int kind() const { return kHostDefined; }
     virtual double value() const { return 0.0; }
+    virtual void apply(int, domain::edges) {}
 };
 
 template <typename T, int rank, pw::arrayTags tag = pw::arrayTags::accelerated>

@@ -81,3 +81,43 @@ def test_reference_ic_package_compiles_and_sets_up(tmp_path):
     rc, out = _run(exe)
     assert rc == 0, out
     assert '"nx": 128, "ny": 128, "nz": 2' in out and '"periodic_slots": 78' in out, out
+
+
+# The reference's own LARE-compatible IC package (src/InitialConditions/LARE,
+# compiled unchanged by tests/cpp/Makefile where the reference tree exists;
+# the binary travels with the checkout).
+LARE_IC = os.path.join(ROOT, "tests", "cpp", "_build", "lare_ic_runner")
+
+
+@pytest.mark.skipif(not os.path.exists(LARE_IC), reason="reference LARE IC driver not built on this machine")
+def test_reference_lare_ic_package_boundary_table():
+    """Its LAREBoundaryConditions (host functions) become device descriptors:
+    the LARE BC_OTHER planes on all 13 variables' 6 edges, except dm in y and
+    z, where the package's dm function does nothing (it only handles x)."""
+    rc, out = _run(LARE_IC, "--check-setup")
+    assert rc == 0, out
+    assert '"lare_other_slots": 74, "none_slots": 4, "dm_y_z_none": true' in out, out
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(LARE_IC), reason="reference LARE IC driver not built on this machine")
+@pytest.mark.parametrize("name", ["ot_lare_12x10x6_s5", "rf_lare_10x8x6_s4"])
+def test_reference_lare_ic_package_on_gpu_matches_reference(name, tmp_path):
+    """The runner with the reference's LARE IC package steps on the GPU and
+    equals the reference's own run of that package (the *_lare_* fixtures:
+    the same seeded state, BC_OTHER on every edge) bit for bit."""
+    import numpy as np
+    from sams_b200 import lare
+    from tests.golden.make_golden import STATE, load
+    z, meta = load(name)
+    nx, ny, nz = meta["nx"], meta["ny"], meta["nz"]
+    out = str(tmp_path / "state.bin")
+    rc, log = _run(LARE_IC, "--run", meta["case"], nx, ny, nz, meta["steps"], meta["seed"], out)
+    assert rc == 0, log
+    assert f'"steps": {meta["steps"]}' in log and '"lare_other_slots": 74' in log, log
+    boxes = np.fromfile(out, dtype="<f8").reshape(lare.NFIELDS, nx + 5, ny + 5, nz + 5)
+    for f in STATE:
+        ref = z[f]
+        m = ~np.isnan(ref)
+        got = boxes[lare.FIELD[f]]
+        assert np.array_equal(got[m], ref[m]), f"{name}: {f} differs (max {np.abs(got[m] - ref[m]).max():.3e})"
