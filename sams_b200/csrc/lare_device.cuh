@@ -238,6 +238,28 @@ __device__ __forceinline__ double limiter_Di(double sign_v, double phi, double d
 
 // Evans-Hawley constrained-transport flux of a transverse face field
 // (vx_by_flux xremap.cpp:269-319 and the five analogues in x/y/zremap.cpp).
+// With the four quotients b/db along the sweep given (fm = bm / dbm, ...):
+// each is the same value at its point for every flux that reads it, so a
+// kernel can form it once per point.
+__device__ __forceinline__ double ct_flux_q(double v_advect, double dt, double fm, double fi, double fp, double fp2,
+                                            double dbi, double dbp, double dci, double dcm, double dcp,
+                                            double cv1i, double cv1p)
+{
+    double o_v = v_advect * dt;
+    double dfm = fi - fm, dfi = fp - fi, dfp = fp2 - fp;
+    double sign_v = (v_advect >= 0.0) ? 1.0 : -1.0;
+    double vad_p = (sign_v + 1.0) * 0.5;
+    double vad_m = 1.0 - vad_p;
+    double fu = fi * vad_p + fp * vad_m;
+    double dfu = dfm * vad_p + dfp * vad_m;
+    double dxcu = dcm * vad_p + dcp * vad_m;
+    double dxbu = cv1i * vad_p + cv1p * vad_m;
+    double dxu = dbi * vad_p + dbp * vad_m;
+    double phi = fabs(o_v) / dxu;
+    double Di = limiter_Di(sign_v, phi, dfi, dfu, dci, dxcu, dxbu);
+    return (fu + Di * (1.0 - phi)) * o_v;
+}
+
 __device__ __forceinline__ double ct_flux(double v_advect, double dt, double bm, double bi, double bp,
                                           double bp2, double dbm, double dbi, double dbp, double dbp2,
                                           double dci, double dcm, double dcp, double cv1i, double cv1p)

@@ -102,6 +102,14 @@ __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int
 // Lagrangian phase
 // ---------------------------------------------------------------------------
 
+// Per-point outputs of one op as another op reads them from global memory:
+// src(arr, q) is array arr at offset q.  (The fused kernels read the same
+// values from a shared-memory ring instead.)
+struct ArraySrc {
+    const double *a[6];
+    __device__ double operator()(int arr, int q) const { return __ldg(a[arr] + q); }
+};
+
 // Sound speed on cells; with resistive MHD also keeps p_e and p_i, which the
 // predictor reads as they were at the start of the step (lagran.cpp:121-123,
 // 606-607): between the two, the resistive sub-steps heat the electrons and
@@ -348,8 +356,22 @@ struct ResistRK {
     {
         set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
+    // outputs: the three edge fluxes and the Ohmic heating rate
+    enum { FX, FY, FZ, CURLB, NOUT };
     template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        double out[NOUT];
+        compute<GEO, P2>(c, i, j, k, out);
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        c.s[S_FLUXX][o] = out[FX];
+        c.s[S_FLUXY][o] = out[FY];
+        c.s[S_FLUXZ][o] = out[FZ];
+        c.s[S_CURLB][o] = out[CURLB];
+    }
+    template <bool GEO, bool P2>
+    __device__ static void compute(const Ctx &c, int i, int j, int k, double *out)
     {
         const Geom &g = c.g;
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
@@ -365,10 +387,10 @@ struct ResistRK {
         double jx = 0.5 * (jx1 + jx2), jy = 0.5 * (jy1 + jy2), jz = 0.5 * (jz1 + jz2);
         double j_local = sqrt(jx * jx + jy * jy + jz * jz);
         double eta = j_local > c.p.j_max ? c.p.eta_bg + c.p.eta0 : c.p.eta_bg;
-        c.s[S_FLUXX][o] = -jx * eta * dxc * 0.5;
-        c.s[S_FLUXY][o] = -jy * eta * dyc * 0.5;
-        c.s[S_FLUXZ][o] = -jz * eta * dzc * 0.5;
-        c.s[S_CURLB][o] = eta * (jx * jx + jy * jy + jz * jz);
+        out[FX] = -jx * eta * dxc * 0.5;
+        out[FY] = -jy * eta * dyc * 0.5;
+        out[FZ] = -jz * eta * dzc * 0.5;
+        out[CURLB] = eta * (jx * jx + jy * jy + jz * jz);
     }
 };
 
@@ -385,34 +407,57 @@ struct ResistB {
     __device__ static void run(const Ctx &c, int last, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const int o = LOFF(i, j, k);
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
-        const RO fx{c.s[S_FLUXX]}, fy{c.s[S_FLUXY]}, fz{c.s[S_FLUXZ]};
-        const double dt = c.sc->dt_sub;
-        double bxo = bx[o], byo = by[o], bzo = bz[o];
         if (last) {
-            c.s[S_B1X][o] = bxo;
-            c.s[S_B1Y][o] = byo;
-            c.s[S_B1Z][o] = bzo;
+            c.s[S_B1X][o] = bx[o];
+            c.s[S_B1Y][o] = by[o];
+            c.s[S_B1Z][o] = bz[o];
         }
+        const ArraySrc src{{c.s[S_FLUXX], c.s[S_FLUXY], c.s[S_FLUXZ], c.s[S_CURLB]}};
+        run_src<P2>(c, i, j, k, src, o, g.sx, g.sy, 1, bx, by, bz);
+    }
+    // The update at (i, j, k) with the fluxes of ResistRK read through
+    // src(array, q) for the cell q = q0 - dx*QX - dy*QY - dz*QZ (dx, dy, dz in
+    // {0, 1}); the new B goes to nbx/nby/nbz[o] (unchanged values included),
+    // the electron energy is updated in place.
+    template <bool P2, class S>
+    __device__ static void run_src(const Ctx &c, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ,
+                                   double *nbx, double *nby, double *nbz)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        struct Arr {
+            const S &s;
+            int a;
+            __device__ double operator[](int q) const { return s(a, q); }
+        };
+        const Arr fx{src, ResistRK::FX}, fy{src, ResistRK::FY}, fz{src, ResistRK::FZ};
+        const double dt = c.sc->dt_sub;
+        const int q = q0, SX = QX, SY = QY;
+        double bxo = __ldg(c.f[SAMS_F_BX] + o), byo = __ldg(c.f[SAMS_F_BY] + o), bzo = __ldg(c.f[SAMS_F_BZ] + o);
         const bool inx = i >= 0 && i <= g.nx, iny = j >= 0 && j <= g.ny, inz = k >= 0 && k <= g.nz;
         const bool inx1 = i >= 1 && i <= g.nx, iny1 = j >= 1 && j <= g.ny, inz1 = k >= 1 && k <= g.nz;
+        double bxn = bxo, byn = byo, bzn = bzo;
         if (inx && iny1 && inz1) {
             double area = c.ax.dyb[j + 2] * c.ax.dzb[k + 2];
-            bx[o] = bxo + div_by<P2>((fz[o] - fz[o - SY] + fz[o - 1] - fz[o - SY - 1] - fy[o] + fy[o - 1] - fy[o - SY] + fy[o - SY - 1]) * dt, area, c.rc.yb * c.rc.zb);
+            bxn = bxo + div_by<P2>((fz[q] - fz[q - SY] + fz[q - QZ] - fz[q - SY - QZ] - fy[q] + fy[q - QZ] - fy[q - SY] + fy[q - SY - QZ]) * dt, area, c.rc.yb * c.rc.zb);
         }
         if (inx1 && iny && inz1) {
             double area = c.ax.dxb[i + 2] * c.ax.dzb[k + 2];
-            by[o] = byo + div_by<P2>((fx[o] - fx[o - 1] + fx[o - SX] - fx[o - SX - 1] - fz[o] + fz[o - SX] - fz[o - 1] + fz[o - SX - 1]) * dt, area, c.rc.xb * c.rc.zb);
+            byn = byo + div_by<P2>((fx[q] - fx[q - QZ] + fx[q - SX] - fx[q - SX - QZ] - fz[q] + fz[q - SX] - fz[q - QZ] + fz[q - SX - QZ]) * dt, area, c.rc.xb * c.rc.zb);
         }
         if (inx1 && iny1 && inz) {
             double area = c.ax.dxb[i + 2] * c.ax.dyb[j + 2];
-            bz[o] = bzo + div_by<P2>((fy[o] - fy[o - SX] + fy[o - SY] - fy[o - SX - SY] - fx[o] + fx[o - SY] - fx[o - SX] + fx[o - SX - SY]) * dt, area, c.rc.xb * c.rc.yb);
+            bzn = bzo + div_by<P2>((fy[q] - fy[q - SX] + fy[q - SY] - fy[q - SX - SY] - fx[q] + fx[q - SY] - fx[q - SX] + fx[q - SX - SY]) * dt, area, c.rc.xb * c.rc.yb);
         }
+        nbx[o] = bxn;
+        nby[o] = byn;
+        nbz[o] = bzn;
         if (inx1 && iny1 && inz1) {
-            const RO curlb{c.s[S_CURLB]};
-            double sum_curlb = curlb[o] + curlb[o - SX] + curlb[o - SY] + curlb[o - SX - SY] +
-                               curlb[o - 1] + curlb[o - SX - 1] + curlb[o - SY - 1] + curlb[o - SX - SY - 1];
+            const Arr curlb{src, ResistRK::CURLB};
+            double sum_curlb = curlb[q] + curlb[q - SX] + curlb[q - SY] + curlb[q - SX - SY] +
+                               curlb[q - QZ] + curlb[q - SX - QZ] + curlb[q - SY - QZ] + curlb[q - SX - SY - QZ];
             double *ee = c.f[SAMS_F_ENERGY_ELECTRON];
             ee[o] += sum_curlb * dt / (8.0 * __ldg(c.f[SAMS_F_RHO] + o));
         }
@@ -427,8 +472,29 @@ struct Pred1 {
     {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
+    // Outputs of one cell, in this order: cv1, b1x*cv1, b1y*cv1, b1z*cv1 and
+    // (where the cell is in 0..n+1 in every dimension, `half_p` set) the
+    // half-step p_e, p_i.  Reads the step-start p_e/p_i of resistive runs
+    // from S_PE/S_PI.
+    enum { CV1, B1X, B1Y, B1Z, PE, PI, NOUT };
     template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int resistive, int i, int j, int k)
+    {
+        double out[NOUT];
+        bool half_p;
+        compute<GEO, P2>(c, resistive, i, j, k, out, half_p);
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        c.s[S_B1X][o] = out[B1X];
+        c.s[S_B1Y][o] = out[B1Y];
+        c.s[S_B1Z][o] = out[B1Z];
+        c.s[S_CV1][o] = out[CV1];
+        if (!half_p) return;
+        c.s[S_PE][o] = out[PE];
+        c.s[S_PI][o] = out[PI];
+    }
+    template <bool GEO, bool P2>
+    __device__ static void compute(const Ctx &c, int resistive, int i, int j, int k, double *out, bool &half_p)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
@@ -474,9 +540,9 @@ struct Pred1 {
 
         double b1x, b1y, b1z;
         if (resistive) {
-            b1x = c.s[S_B1X][o];
-            b1y = c.s[S_B1Y][o];
-            b1z = c.s[S_B1Z][o];
+            b1x = __ldg(c.s[S_B1X] + o);
+            b1y = __ldg(c.s[S_B1Y] + o);
+            b1z = __ldg(c.s[S_B1Z] + o);
         } else {
             const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
             b1x = 0.5 * (bx[o] + bx[o - SX]);
@@ -489,23 +555,24 @@ struct Pred1 {
         b1x = (b1x + w3 * dt / 2.0) / (1.0 + dv);
         b1y = (b1y + w4 * dt / 2.0) / (1.0 + dv);
         b1z = (b1z + w5 * dt / 2.0) / (1.0 + dv);
-        c.s[S_B1X][o] = b1x * cv1;
-        c.s[S_B1Y][o] = b1y * cv1;
-        c.s[S_B1Z][o] = b1z * cv1;
-        c.s[S_CV1][o] = cv1;
+        out[B1X] = b1x * cv1;
+        out[B1Y] = b1y * cv1;
+        out[B1Z] = b1z * cv1;
+        out[CV1] = cv1;
 
-        if (i < 0 || i > g.nx + 1 || j < 0 || j > g.ny + 1 || k < 0 || k > g.nz + 1) return;
+        half_p = !(i < 0 || i > g.nx + 1 || j < 0 || j > g.ny + 1 || k < 0 || k > g.nz + 1);
+        if (!half_p) return;
         const double gm = c.p.gamma;
         double rho = __ldg(c.f[SAMS_F_RHO] + o), ee = __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
         double ei = __ldg(c.f[SAMS_F_ENERGY_ION] + o);
-        double pe = resistive ? c.s[S_PE][o] : (gm - 1.0) * rho * ee;
-        double pi = resistive ? c.s[S_PI][o] : (gm - 1.0) * rho * ei;
+        double pe = resistive ? __ldg(c.s[S_PE] + o) : (gm - 1.0) * rho * ee;
+        double pi = resistive ? __ldg(c.s[S_PI] + o) : (gm - 1.0) * rho * ei;
         double dvv = div_by<P2>(cv1, vol, c.rc.cv) - 1.0;
         double e1_e = ee - pe * dvv / rho;
         double e1_i = ei - pi * dvv / rho;
         e1_i += __ldg(c.s[S_VH] + o) * dt / 2.0 / rho;
-        c.s[S_PE][o] = e1_e * (gm - 1.0) * rho * vol / cv1;
-        c.s[S_PI][o] = e1_i * (gm - 1.0) * rho * vol / cv1;
+        out[PE] = e1_e * (gm - 1.0) * rho * vol / cv1;
+        out[PI] = e1_i * (gm - 1.0) * rho * vol / cv1;
     }
 };
 
@@ -521,9 +588,23 @@ struct Pred2 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const RO pe{c.s[S_PE]}, pi{c.s[S_PI]}, cv1{c.s[S_CV1]};
-        const RO bx1{c.s[S_B1X]}, by1{c.s[S_B1Y]}, bz1{c.s[S_B1Z]};
+        const ArraySrc src{{c.s[S_CV1], c.s[S_B1X], c.s[S_B1Y], c.s[S_B1Z], c.s[S_PE], c.s[S_PI]}};
+        run_src<GEO, P2>(c, i, j, k, src, LOFF(i, j, k), g.sx, g.sy, 1);
+    }
+    // The node's update with Pred1's outputs read through src(array, q) for
+    // the cell q = q0 + dx*QX + dy*QY + dz*QZ (dx, dy, dz in {0, 1}).
+    template <bool GEO, bool P2, class S>
+    __device__ static void run_src(const Ctx &c, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        struct Arr {
+            const S &s;
+            int a;
+            __device__ double operator[](int q) const { return s(a, q); }
+        };
+        const Arr pe{src, Pred1::PE}, pi{src, Pred1::PI}, cv1{src, Pred1::CV1};
+        const Arr bx1{src, Pred1::B1X}, by1{src, Pred1::B1Y}, bz1{src, Pred1::B1Z};
         const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
         // metric factors (lagran.cpp:627-630; all 1.0 in Cartesian geometry)
         const bool geo = GEO && c.p.geometry != 0;
@@ -538,8 +619,8 @@ struct Pred2 {
             h3c = c.gf.hzc[h2_index(c, i, j)];
         }
         const double dhy = geo ? h2c * dy : dy, dhz = geo ? h3c * dz : dz;
-        const int q0 = o, qx = o + SX, qy = o + SY, qz = o + 1, qxy = o + SX + SY, qxz = o + SX + 1,
-                        qyz = o + SY + 1, qxyz = o + SX + SY + 1;
+        const int qx = q0 + QX, qy = q0 + QY, qz = q0 + QZ, qxy = q0 + QX + QY, qxz = q0 + QX + QZ,
+                  qyz = q0 + QY + QZ, qxyz = q0 + QX + QY + QZ;
         double pp = pe[q0] + pi[q0], ppx = pe[qx] + pi[qx], ppy = pe[qy] + pi[qy], ppz = pe[qz] + pi[qz];
         double ppxy = pe[qxy] + pi[qxy], ppxz = pe[qxz] + pi[qxz], ppyz = pe[qyz] + pi[qyz], ppxyz = pe[qxyz] + pi[qxyz];
         double w1 = pp + ppy + ppz + ppyz;
@@ -985,6 +1066,64 @@ struct SweepMass {
         double v = face_velocity<DIR>(c, o);
         c.f[SAMS_F_DM][o] = mass_flux(v, c.sc->dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d], rho[o], rho[o + d],
                                       rho[o + 2 * d], cvc1[o], cvc1[o - d], cvc1[o + d], cv1[o], cv1[o + d]);
+    }
+};
+
+// SweepCT and SweepMass of one sweep in one kernel (k_ctmass): every
+// quotient b/db of the CT fluxes is formed once per point into a window store
+// and read by the four fluxes along the sweep that use it (the separate
+// kernel forms each four times).  quot() at one point along the sweep, then
+// fluxes() at the window's own points.
+template <int DIR>
+struct SweepCTMass {
+    enum { F1, F2, DB1, DB2, NARR };  // the two quotients and their db averages
+    // t1 / t2: transverse offset of the db1 sample averaged for flux 1 / 2;
+    // va1 / va2: offset of the second v1 sample of its advection velocity
+    __device__ static void offsets(const Geom &g, int &t1, int &t2, int &va1, int &va2)
+    {
+        if (DIR == 0) { t1 = g.sy; va1 = -1; t2 = 1; va2 = -g.sy; }
+        else if (DIR == 1) { t1 = g.sx; va1 = -1; t2 = 1; va2 = -g.sx; }
+        else { t1 = g.sx; va1 = -g.sy; t2 = g.sy; va2 = -g.sx; }
+    }
+    template <class A>
+    __device__ static void quot(const Ctx &c, int i, int j, int k, A st)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        int t1, t2, va1, va2;
+        offsets(g, t1, t2, va1, va2);
+        const RO db1{c.s[S_R_DB1]};
+        const RO b1{c.f[DIR == 0 ? SAMS_F_BY : SAMS_F_BX]}, b2{c.f[DIR == 2 ? SAMS_F_BY : SAMS_F_BZ]};
+        const double dba1 = (db1[o] + db1[o + t1]) * 0.5, dba2 = (db1[o] + db1[o + t2]) * 0.5;
+        st.put(F1, b1[o] / dba1);
+        st.put(F2, b2[o] / dba2);
+        st.put(DB1, dba1);
+        st.put(DB2, dba2);
+    }
+    // CT fluxes where `ct` ((i, j, k) in 0..n), the mass flux everywhere it
+    // is called (0..n along the sweep, 0..n+1 across)
+    template <bool GEO, class A>
+    __device__ static void fluxes(const Ctx &c, int i, int j, int k, A st, bool ct)
+    {
+        const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        const int d = dir_stride(g, DIR);
+        const double dt = c.sc->dt;
+        const RO cvc1{c.s[S_R_CVC1]}, cv1{c.s[S_R_CV1]};
+        const double dci = cvc1[o], dcm = cvc1[o - d], dcp = cvc1[o + d], cvi = cv1[o], cvp = cv1[o + d];
+        if (ct) {
+            int t1, t2, va1, va2;
+            offsets(g, t1, t2, va1, va2);
+            const RO v1{c.f[SAMS_F_VX1 + DIR]};
+            const double v1o = v1[o];
+            c.s[S_R_CT1][o] = ct_flux_q((v1o + v1[o + va1]) * 0.5, dt, st.get(F1, -1), st.get(F1, 0), st.get(F1, 1),
+                                        st.get(F1, 2), st.get(DB1, 0), st.get(DB1, 1), dci, dcm, dcp, cvi, cvp);
+            c.s[S_R_CT2][o] = ct_flux_q((v1o + v1[o + va2]) * 0.5, dt, st.get(F2, -1), st.get(F2, 0), st.get(F2, 1),
+                                        st.get(F2, 2), st.get(DB2, 0), st.get(DB2, 1), dci, dcm, dcp, cvi, cvp);
+        }
+        const RO rho{c.f[SAMS_F_RHO]};
+        c.f[SAMS_F_DM][o] = mass_flux(face_velocity<DIR>(c, o), dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d],
+                                      rho[o], rho[o + d], rho[o + 2 * d], dci, dcm, dcp, cvi, cvp);
     }
 };
 

@@ -104,6 +104,192 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::Swee
         if (on) F::stage_c(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w);
 }
 
+// The predictor (ops::Pred1 then ops::Pred2) in one kernel.  A block owns
+// kMK x kMJ nodes of a y-z plane (k fastest) and a chunk of kMI planes along
+// x, and marches along x: for each plane i it computes Pred1 for the cells of
+// plane i+1 that its nodes read (its kMJ+1 x kMK+1 cells: the +1 halo in y
+// and z is recomputed by the neighbouring block too) into a ring of three
+// planes in shared memory, then Pred2 for its nodes of plane i from the
+// ring.  cv1 and the half-step B never go to global memory.  The half-step
+// p_e and p_i of the block's own cells go to pe_out / pi_out: in resistive
+// runs Pred1 reads the step-start p_e / p_i at cells that other blocks own,
+// so those arrays cannot be overwritten in place.
+constexpr int kMK = 32, kMJ = 8, kMI = 16, kMThreads = kMK * kMJ;
+constexpr int kRP = (kMK + 1) * (kMJ + 1);  // cells of one ring plane
+
+struct RingSrc {
+    const double *ring;
+    __device__ double operator()(int arr, int q) const { return ring[arr * 3 * kRP + q]; }
+};
+
+template <bool GEO, bool P2>
+__global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistive, double *pe_out, double *pi_out)
+{
+    using P1 = ops::Pred1;
+    extern __shared__ double ring[];  // [P1::NOUT][3 planes][kRP]
+    const Geom &g = c.g;
+    const int nkt = (g.nz + kMK) / kMK, njt = (g.ny + kMJ) / kMJ;  // tiles over nodes 0..n
+    int b = (int)blockIdx.x;
+    const int tk = b % nkt;
+    b /= nkt;
+    const int tj = b % njt;
+    const int i0 = (b / njt) * kMI, i1 = min(i0 + kMI - 1, g.nx);
+    const int k0 = tk * kMK, j0 = tj * kMJ;
+    const int t = (int)threadIdx.x;
+    // Pred1 at the block's cells of plane i (cells 0..n+1: what Pred2 reads)
+    auto produce = [&](int i) {
+        const int slot = i % 3;
+        for (int p = t; p < kRP; p += kMThreads) {
+            const int pj = p / (kMK + 1), pk = p - pj * (kMK + 1);
+            const int j = j0 + pj, k = k0 + pk;
+            if (j > g.ny + 1 || k > g.nz + 1) continue;
+            double out[P1::NOUT];
+            bool half_p;
+            P1::compute<GEO, P2>(c, resistive, i, j, k, out, half_p);
+#pragma unroll
+            for (int a = 0; a < P1::NOUT; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
+            if (pj < kMJ && pk < kMK && i <= i1 && j <= g.ny && k <= g.nz) {
+                const int o = box_off(g, i, j, k);
+                pe_out[o] = out[P1::PE];
+                pi_out[o] = out[P1::PI];
+            }
+        }
+    };
+    const int kc = t % kMK, jc = t / kMK;
+    const int j = j0 + jc, k = k0 + kc;
+    const bool on = j <= g.ny && k <= g.nz;
+    const RingSrc src{ring};
+    produce(i0);
+    for (int i = i0; i <= i1; ++i) {
+        produce(i + 1);
+        __syncthreads();  // the ring's planes i and i+1 are complete
+        if (on) {
+            const int s0 = i % 3, s1 = (i + 1) % 3;
+            ops::Pred2::run_src<GEO, P2>(c, i, j, k, src, s0 * kRP + jc * (kMK + 1) + kc, (s1 - s0) * kRP, kMK + 1, 1);
+        }
+        // three ring planes: the next iteration's producer writes the plane
+        // this one read as i-1, which no thread reads after this barrier
+    }
+}
+
+// One resistive sub-step (ops::ResistRK then ops::ResistB) in one kernel,
+// out of place for B.  A block owns kMK x kMJ points of a y-z plane of the
+// whole box (-2..n+2) and a chunk of kMI planes along x, and marches along x:
+// ResistRK for the cells of plane i that its points read (the -1 halo in y
+// and z is recomputed by the neighbouring block) goes into a ring of three
+// planes in shared memory, then ResistB for its points of plane i reads the
+// ring's planes i-1 and i.  ResistRK reads B at +1 neighbours that other
+// blocks update, so the new B goes to nbx/nby/nbz (every box point: updated
+// or copied); the electron energy is updated in place (nothing else reads
+// it here).
+template <bool GEO, bool P2>
+__global__ void __launch_bounds__(kMThreads, 4) k_resist_march(Ctx c, double *nbx, double *nby, double *nbz)
+{
+    using RK = ops::ResistRK;
+    extern __shared__ double ring[];  // [RK::NOUT][3 planes][kRP]
+    const Geom &g = c.g;
+    const int nkt = (g.nz + 4 + kMK) / kMK, njt = (g.ny + 4 + kMJ) / kMJ;  // tiles over -2..n+2
+    int b = (int)blockIdx.x;
+    const int tk = b % nkt;
+    b /= nkt;
+    const int tj = b % njt;
+    const int i0 = -2 + (b / njt) * kMI, i1 = min(i0 + kMI - 1, g.nx + 2);
+    const int k0 = -2 + tk * kMK, j0 = -2 + tj * kMJ;
+    const int t = (int)threadIdx.x;
+    // ResistRK at the block's cells of plane i (ring index (j - j0 + 1, k - k0 + 1)),
+    // where it is defined (0..n)
+    auto produce = [&](int i) {
+        if (i < 0 || i > g.nx) return;
+        const int slot = (i + 6) % 3;
+        for (int p = t; p < kRP; p += kMThreads) {
+            const int pj = p / (kMK + 1), pk = p - pj * (kMK + 1);
+            const int j = j0 - 1 + pj, k = k0 - 1 + pk;
+            if (j < 0 || j > g.ny || k < 0 || k > g.nz) continue;
+            double out[RK::NOUT];
+            RK::compute<GEO, P2>(c, i, j, k, out);
+#pragma unroll
+            for (int a = 0; a < RK::NOUT; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
+        }
+    };
+    const int kc = t % kMK, jc = t / kMK;
+    const int j = j0 + jc, k = k0 + kc;
+    const bool on = j <= g.ny + 2 && k <= g.nz + 2;
+    const RingSrc src{ring};
+    produce(i0 - 1);
+    for (int i = i0; i <= i1; ++i) {
+        produce(i);
+        __syncthreads();  // the ring's planes i-1 and i are complete
+        if (on) {
+            const int s0 = (i + 6) % 3, sm = (i + 5) % 3;
+            ops::ResistB::run_src<P2>(c, i, j, k, src, s0 * kRP + (jc + 1) * (kMK + 1) + (kc + 1), (s0 - sm) * kRP,
+                                      kMK + 1, 1, nbx, nby, nbz);
+        }
+    }
+}
+
+// SweepCT + SweepMass of the x or y sweep (ops::SweepCTMass<DIR>) over
+// windows of kWinK adjacent k times kWinS own points along DIR, for one value
+// a of the third index (j for x, i for y).  The CT quotients of the window's
+// points and of a halo of one before and two after go to shared memory first.
+// CT fluxes where a and k are in 0..n, mass fluxes where they are in 0..n+1.
+template <int DIR, bool GEO>
+__global__ void __launch_bounds__(ops::kWinThreads, 4) k_ctmass(Ctx c)
+{
+    using F = ops::SweepCTMass<DIR>;
+    constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
+    extern __shared__ double csm[];
+    const Geom &g = c.g;
+    const int nd = DIR == 0 ? g.nx : g.ny, na = DIR == 0 ? g.ny : g.nx;
+    const int nkt = (g.nz + 1 + TK) / TK, nwin = (nd + ops::kWinS) / ops::kWinS;
+    const int b = (int)blockIdx.x;
+    const int win = b % nwin, kt = (b / nwin) % nkt, a = b / (nwin * nkt);
+    const int s0 = win * ops::kWinS, s1 = min(s0 + ops::kWinS - 1, nd);
+    const int kc = (int)threadIdx.x % TK, sl = (int)threadIdx.x / TK;
+    const int k = kt * TK + kc;
+    const bool ct = a <= na && k <= g.nz, mass = k <= g.nz + 1;
+    auto at = [&](int s) { return ops::WinStore{csm, s - s0 + 1, kc}; };
+    if (ct)
+        for (int s = s0 - 1 + sl; s <= s1 + 2; s += TS) F::quot(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s));
+    __syncthreads();
+    if (mass)
+        for (int s = s0 + sl; s <= s1; s += TS)
+            F::template fluxes<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), ct);
+}
+
+// SweepCT + SweepMass of the z sweep: kZRows lines (i, j) in 0..nx+1 x
+// 0..ny+1 per block (CT fluxes on the lines in 0..n), 32 own k in 0..nz each;
+// the quotients of k0-1 .. k0+34 (up to nz+2) of each line go to shared
+// memory first.
+constexpr int kZRows = 8, kZSpan = 32 + 3;
+struct ZRowStore {
+    double *sm;
+    int at;
+    __device__ double get(int a, int ds) const { return sm[a * (kZRows * kZSpan) + at + ds]; }
+    __device__ void put(int a, double v) const { sm[a * (kZRows * kZSpan) + at] = v; }
+};
+
+template <bool GEO>
+__global__ void __launch_bounds__(256, 4) k_ctmass_z(Ctx c)
+{
+    using F = ops::SweepCTMass<2>;
+    __shared__ double zsm[F::NARR * kZRows * kZSpan];
+    const Geom &g = c.g;
+    const int r = (int)threadIdx.x / 32, kc = (int)threadIdx.x % 32;
+    const long long line = (long long)blockIdx.x * kZRows + r;
+    const bool on = line < (long long)(g.nx + 2) * (g.ny + 2);
+    const int i = on ? (int)(line / (g.ny + 2)) : 0, j = on ? (int)(line % (g.ny + 2)) : 0;
+    const int k0 = (int)blockIdx.y * 32;
+    const bool ct = on && i <= g.nx && j <= g.ny;
+    if (ct)
+        for (int kk = kc; kk < kZSpan; kk += 32) {
+            const int k = k0 - 1 + kk;
+            if (k <= g.nz + 2) F::quot(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk});
+        }
+    __syncthreads();
+    const int k = k0 + kc;  // along the sweep: 0..nz for both fluxes
+    if (on && k <= g.nz) F::fluxes<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kc + 1}, ct);
+}
+
 // The points of the out-of-place sweep's arrays it does not compute (rho and
 // energies outside 1..n, velocities outside 0..n in some dimension): copied
 // from the solve's arrays, so the new arrays are complete boxes.  One
@@ -622,6 +808,80 @@ int Solver::setup_psweep()
     return SAMS_OK;
 }
 
+// Pred1 + Pred2 fused (k_pred_march); the half-step pressures land in the
+// S_CS / S_CSV arrays (free from here to the remap), whose slots then swap
+// with S_PE / S_PI.
+void Solver::launch_pred(int resistive)
+{
+    const Geom &g = ctx_.g;
+    const long long blocks = (long long)((g.nz + kMK) / kMK) * ((g.ny + kMJ) / kMJ) * ((g.nx + kMI) / kMI);
+    const size_t smem = (size_t)ops::Pred1::NOUT * 3 * kRP * sizeof(double);
+    double *pe = ctx_.s[S_CS], *pi = ctx_.s[S_CSV];
+    if (ctx_.p.geometry)
+        k_pred_march<true, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, resistive, pe, pi);
+    else if (ctx_.p.pow2)
+        k_pred_march<false, true><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, resistive, pe, pi);
+    else
+        k_pred_march<false, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, resistive, pe, pi);
+    ++launches_;
+    std::swap(ctx_.s[S_PE], ctx_.s[S_CS]);
+    std::swap(ctx_.s[S_PI], ctx_.s[S_CSV]);
+}
+
+// One resistive sub-step fused (k_resist_march): the new B goes to the
+// S_CS / S_CSV / S_CV1 arrays (free during the sub-steps), whose slots then
+// swap with the field's, so after the two sub-steps B is back in its own
+// arrays and those three slots hold B as it was at the start of the last
+// sub-step: the predictor's b1 (resistive_effects' copy, lagran.cpp:482-484).
+void Solver::launch_resist(bool last)
+{
+    const Geom &g = ctx_.g;
+    const long long blocks =
+        (long long)((g.nz + 4 + kMK) / kMK) * ((g.ny + 4 + kMJ) / kMJ) * ((g.nx + 4 + kMI) / kMI);
+    const size_t smem = (size_t)ops::ResistRK::NOUT * 3 * kRP * sizeof(double);
+    double *nb[3] = {ctx_.s[S_CS], ctx_.s[S_CSV], ctx_.s[S_CV1]};
+    if (ctx_.p.geometry)
+        k_resist_march<true, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, nb[0], nb[1], nb[2]);
+    else if (ctx_.p.pow2)
+        k_resist_march<false, true><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, nb[0], nb[1], nb[2]);
+    else
+        k_resist_march<false, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, nb[0], nb[1], nb[2]);
+    ++launches_;
+    std::swap(ctx_.f[SAMS_F_BX], ctx_.s[S_CS]);
+    std::swap(ctx_.f[SAMS_F_BY], ctx_.s[S_CSV]);
+    std::swap(ctx_.f[SAMS_F_BZ], ctx_.s[S_CV1]);
+    if (last) {
+        std::swap(ctx_.s[S_B1X], ctx_.s[S_CS]);
+        std::swap(ctx_.s[S_B1Y], ctx_.s[S_CSV]);
+        std::swap(ctx_.s[S_B1Z], ctx_.s[S_CV1]);
+    }
+}
+
+// SweepCT + SweepMass of one sweep (k_ctmass / k_ctmass_z).
+template <int DIR>
+void Solver::launch_ctmass()
+{
+    const Geom &g = ctx_.g;
+    if (DIR == 2) {
+        const long long lines = (long long)(g.nx + 2) * (g.ny + 2);
+        dim3 grid((unsigned)ceil_div(lines, kZRows), (unsigned)ceil_div(g.nz + 1, 32));
+        if (ctx_.p.geometry)
+            k_ctmass_z<true><<<grid, 256, 0, stream_>>>(ctx_);
+        else
+            k_ctmass_z<false><<<grid, 256, 0, stream_>>>(ctx_);
+    } else {
+        const int nd = DIR == 0 ? g.nx : g.ny, na = DIR == 0 ? g.ny : g.nx;
+        const long long blocks = (long long)(na + 2) * ((g.nz + 1 + ops::kWinK) / ops::kWinK) *
+                                 ((nd + ops::kWinS) / ops::kWinS);
+        const size_t smem = (size_t)ops::SweepCTMass<DIR>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
+        if (ctx_.p.geometry)
+            k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_);
+        else
+            k_ctmass<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_);
+    }
+    ++launches_;
+}
+
 template <class Op>
 void Solver::launch(int arg)
 {
@@ -726,13 +986,11 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     ++launches_;
     if (resistive) {
         for (int sub = 0; sub < 2; ++sub) {
-            launch<ops::ResistRK>(0);
-            launch<ops::ResistB>(sub == 1 ? 1 : 0);
+            launch_resist(sub == 1);
             bc_fill(FM_BFIELD | FM_ENERGY);
         }
     }
-    launch<ops::Pred1>(resistive);
-    launch<ops::Pred2>(0);
+    launch_pred(resistive);
     bc_fill(FM_REMAPV);
     mark(1);
     // ---- corrector ----
@@ -745,9 +1003,8 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     launch<ops::BScale>(0);
     launch<ops::SweepVol<0>>(0);
     launch<ops::SweepCvc>(0);
-    launch<ops::SweepCT<0>>(0);
+    launch_ctmass<0>();
     launch<ops::SweepCTUpd<0>>(0);
-    launch<ops::SweepMass<0>>(0);
     bc_fill_dim(FM_DM, 0);
     if (!p_.rke && psweep_ok_) {
         launch_psweep<0>();
@@ -764,9 +1021,8 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     mark(3);
     launch<ops::SweepVol<1>>(0);
     launch<ops::SweepCvc>(0);
-    launch<ops::SweepCT<1>>(0);
+    launch_ctmass<1>();
     launch<ops::SweepCTUpd<1>>(0);
-    launch<ops::SweepMass<1>>(0);
     bc_fill_dim(FM_DM, 1);
     if (!p_.rke && psweep_ok_) {
         launch_psweep<1>();
@@ -783,9 +1039,8 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     mark(4);
     launch<ops::SweepVol<2>>(0);
     launch<ops::SweepCvc>(0);
-    launch<ops::SweepCT<2>>(0);
+    launch_ctmass<2>();
     launch<ops::SweepCTUpd<2>>(0);
-    launch<ops::SweepMass<2>>(0);
     bc_fill_dim(FM_DM, 2);
     if (!p_.rke && ctx_.g.nz + 4 <= kZThreads) {
         const Geom &g = ctx_.g;

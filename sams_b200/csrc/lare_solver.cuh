@@ -103,6 +103,9 @@ private:
     bool all_periodic(unsigned mask) const;
     template <class Op> void launch(int arg);
     template <int DIR> void launch_psweep();
+    void launch_pred(int resistive);
+    void launch_resist(bool last);
+    template <int DIR> void launch_ctmass();
     int setup_psweep();
     int staging(double **out);
     void free_all();

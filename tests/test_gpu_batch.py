@@ -136,3 +136,22 @@ def test_batch_with_lare_other_bcs_equals_solo():
         _check_equal(bt, sid, case, n, ref, st)
     bt.close()
 
+
+
+def test_config3_batch_equals_each_plain_run():
+    """The batched workload at its configured size: 64 Orszag-Tang solves
+    n x n x 4, n = round(64 * 8^u) (u seeded), B0 uniform in [0.5, 1.5]/sqrt(4 pi),
+    3 batched steps; every solve equals its own plain run bit for bit."""
+    import math
+    rng = np.random.default_rng(2024)
+    ns = [int(round(64 * 8 ** u)) for u in rng.random(64)]
+    b0s = rng.uniform(0.5, 1.5, 64) / math.sqrt(4 * math.pi)
+    steps = 3
+    bt = lare.Batch()
+    ids = [_add(bt, "ot", (n, n, 4), 1, b0) for n, b0 in zip(ns, b0s)]
+    bt.step(steps, graph=True)
+    bt.synchronize()
+    for sid, n, b0 in zip(ids, ns, b0s):
+        ref, st = _solo("ot", (n, n, 4), 1, b0, steps)
+        _check_equal(bt, sid, "ot", (n, n, 4), ref, st)
+    bt.close()

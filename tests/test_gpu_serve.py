@@ -108,3 +108,29 @@ def test_cancel_queued_and_running_requests():
     for t in (long_run, queued, last):
         srv.release(t)
     srv.close()
+
+
+def test_served_mix_with_a_192_cube_equals_solo():
+    """A config-4-shaped mix (random-field cubes, resistive, one of edge 192)
+    arriving while others run, under a cell cap that makes the 192^3 solve
+    wait for room: each result equals its solo run bit for bit."""
+    reqs = [("rf", (64, 64, 64), 6, 11), ("rf", (192, 192, 192), 4, 12), ("rf", (32, 32, 32), 9, 13),
+            ("rf", (96, 96, 96), 5, 14)]
+    srv = lare.Server(40 << 30, max_cells=8_000_000)
+    tickets, outs = [], []
+    for case, n, steps, seed in reqs:
+        p, b = lare.case_setup(case, *n)
+        out = [np.zeros(lare.box_shape(*n)) for _ in range(9)]
+        tickets.append(srv.submit(p, b, lare.case_fields(case, p, seed=seed), steps, out))
+        outs.append(out)
+        time.sleep(0.02)
+    srv.drain(600)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    for t, out, (case, n, steps, seed) in zip(tickets, outs, reqs):
+        assert srv.poll(t)[0] == "done"
+        ref = _solo(case, n, steps, seed)
+        for q, f in enumerate(STATE):
+            sl = lare.field_slices(f, *n)
+            assert np.array_equal(out[q][sl], ref[f][sl]), f"{case}{n} {f}"
+    srv.close()
