@@ -1416,7 +1416,7 @@ struct LineStore {
 // points along the line, plus stage A's halo of two points before and one
 // after and stage B's of one before.  Array a of the window at
 // sm[((a * P) + p) * kWinK + kc], p = s - s0 + 2, P = kWinS + 3.
-constexpr int kWinK = 32, kWinS = 24, kWinThreads = 256;  // 48 KB of shared memory: 4 blocks per SM
+constexpr int kWinK = 32, kWinS = 21, kWinThreads = 256;  // 43 KB of shared memory: 4 blocks per SM (window tuned on B200)
 struct WinStore {
     double *sm;
     int at, kc;

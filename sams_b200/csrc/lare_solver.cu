@@ -114,8 +114,13 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::Swee
 // p_e and p_i of the block's own cells go to pe_out / pi_out: in resistive
 // runs Pred1 reads the step-start p_e / p_i at cells that other blocks own,
 // so those arrays cannot be overwritten in place.
-constexpr int kMK = 32, kMJ = 8, kMI = 16, kMThreads = kMK * kMJ;
+// The ring plane is (kMK+1) x (kMJ+1) cells, one per thread of a block of
+// kMThreads: 32 x 9, nine full warps, so the producer is one pass; the
+// consumer maps thread t to (t / (kMK+1), t % (kMK+1)) and leaves the last
+// lane of each row and the last row idle.
+constexpr int kMK = 31, kMJ = 8, kMI = 16;
 constexpr int kRP = (kMK + 1) * (kMJ + 1);  // cells of one ring plane
+constexpr int kMThreads = (kRP + 31) / 32 * 32;
 
 struct RingSrc {
     const double *ring;
@@ -155,9 +160,9 @@ __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistiv
             }
         }
     };
-    const int kc = t % kMK, jc = t / kMK;
+    const int kc = t % (kMK + 1), jc = t / (kMK + 1);
     const int j = j0 + jc, k = k0 + kc;
-    const bool on = j <= g.ny && k <= g.nz;
+    const bool on = kc < kMK && jc < kMJ && j <= g.ny && k <= g.nz;
     const RingSrc src{ring};
     produce(i0);
     for (int i = i0; i <= i1; ++i) {
@@ -183,7 +188,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistiv
 // or copied); the electron energy is updated in place (nothing else reads
 // it here).
 template <bool GEO, bool P2>
-__global__ void __launch_bounds__(kMThreads, 4) k_resist_march(Ctx c, double *nbx, double *nby, double *nbz)
+__global__ void __launch_bounds__(kMThreads, 5) k_resist_march(Ctx c, double *nbx, double *nby, double *nbz)
 {
     using RK = ops::ResistRK;
     extern __shared__ double ring[];  // [RK::NOUT][3 planes][kRP]
@@ -211,9 +216,9 @@ __global__ void __launch_bounds__(kMThreads, 4) k_resist_march(Ctx c, double *nb
             for (int a = 0; a < RK::NOUT; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
         }
     };
-    const int kc = t % kMK, jc = t / kMK;
+    const int kc = t % (kMK + 1), jc = t / (kMK + 1);
     const int j = j0 + jc, k = k0 + kc;
-    const bool on = j <= g.ny + 2 && k <= g.nz + 2;
+    const bool on = kc < kMK && jc < kMJ && j <= g.ny + 2 && k <= g.nz + 2;
     const RingSrc src{ring};
     produce(i0 - 1);
     for (int i = i0; i <= i1; ++i) {
@@ -232,22 +237,31 @@ __global__ void __launch_bounds__(kMThreads, 4) k_resist_march(Ctx c, double *nb
 // a of the third index (j for x, i for y).  The CT quotients of the window's
 // points and of a halo of one before and two after go to shared memory first.
 // CT fluxes where a and k are in 0..n, mass fluxes where they are in 0..n+1.
+constexpr int kCtS = 21;              // own points of a window along the sweep (tuned on B200)
+constexpr int kCtP = kCtS + 3;         // with the quotient halo (one before, two after)
+struct CtStore {
+    double *sm;
+    int at, kc;
+    __device__ double get(int a, int ds) const { return sm[(a * kCtP + at + ds) * ops::kWinK + kc]; }
+    __device__ void put(int a, double v) const { sm[(a * kCtP + at) * ops::kWinK + kc] = v; }
+};
+
 template <int DIR, bool GEO>
-__global__ void __launch_bounds__(ops::kWinThreads, 4) k_ctmass(Ctx c)
+__global__ void __launch_bounds__(ops::kWinThreads, 6) k_ctmass(Ctx c)
 {
     using F = ops::SweepCTMass<DIR>;
     constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
     extern __shared__ double csm[];
     const Geom &g = c.g;
     const int nd = DIR == 0 ? g.nx : g.ny, na = DIR == 0 ? g.ny : g.nx;
-    const int nkt = (g.nz + 1 + TK) / TK, nwin = (nd + ops::kWinS) / ops::kWinS;
+    const int nkt = (g.nz + 1 + TK) / TK, nwin = (nd + kCtS) / kCtS;
     const int b = (int)blockIdx.x;
     const int win = b % nwin, kt = (b / nwin) % nkt, a = b / (nwin * nkt);
-    const int s0 = win * ops::kWinS, s1 = min(s0 + ops::kWinS - 1, nd);
+    const int s0 = win * kCtS, s1 = min(s0 + kCtS - 1, nd);
     const int kc = (int)threadIdx.x % TK, sl = (int)threadIdx.x / TK;
     const int k = kt * TK + kc;
     const bool ct = a <= na && k <= g.nz, mass = k <= g.nz + 1;
-    auto at = [&](int s) { return ops::WinStore{csm, s - s0 + 1, kc}; };
+    auto at = [&](int s) { return CtStore{csm, s - s0 + 1, kc}; };
     if (ct)
         for (int s = s0 - 1 + sl; s <= s1 + 2; s += TS) F::quot(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s));
     __syncthreads();
@@ -260,7 +274,7 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_ctmass(Ctx c)
 // 0..ny+1 per block (CT fluxes on the lines in 0..n), 32 own k in 0..nz each;
 // the quotients of k0-1 .. k0+34 (up to nz+2) of each line go to shared
 // memory first.
-constexpr int kZRows = 8, kZSpan = 32 + 3;
+constexpr int kZRows = 8, kZOwn = 64, kZSpan = kZOwn + 3;
 struct ZRowStore {
     double *sm;
     int at;
@@ -269,7 +283,7 @@ struct ZRowStore {
 };
 
 template <bool GEO>
-__global__ void __launch_bounds__(256, 4) k_ctmass_z(Ctx c)
+__global__ void __launch_bounds__(256, 6) k_ctmass_z(Ctx c)
 {
     using F = ops::SweepCTMass<2>;
     __shared__ double zsm[F::NARR * kZRows * kZSpan];
@@ -278,7 +292,7 @@ __global__ void __launch_bounds__(256, 4) k_ctmass_z(Ctx c)
     const long long line = (long long)blockIdx.x * kZRows + r;
     const bool on = line < (long long)(g.nx + 2) * (g.ny + 2);
     const int i = on ? (int)(line / (g.ny + 2)) : 0, j = on ? (int)(line % (g.ny + 2)) : 0;
-    const int k0 = (int)blockIdx.y * 32;
+    const int k0 = (int)blockIdx.y * kZOwn;
     const bool ct = on && i <= g.nx && j <= g.ny;
     if (ct)
         for (int kk = kc; kk < kZSpan; kk += 32) {
@@ -286,8 +300,10 @@ __global__ void __launch_bounds__(256, 4) k_ctmass_z(Ctx c)
             if (k <= g.nz + 2) F::quot(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk});
         }
     __syncthreads();
-    const int k = k0 + kc;  // along the sweep: 0..nz for both fluxes
-    if (on && k <= g.nz) F::fluxes<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kc + 1}, ct);
+    for (int kk = kc; kk < kZOwn; kk += 32) {
+        const int k = k0 + kk;  // along the sweep: 0..nz for both fluxes
+        if (on && k <= g.nz) F::fluxes<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk + 1}, ct);
+    }
 }
 
 // The points of the out-of-place sweep's arrays it does not compute (rho and
@@ -864,7 +880,7 @@ void Solver::launch_ctmass()
     const Geom &g = ctx_.g;
     if (DIR == 2) {
         const long long lines = (long long)(g.nx + 2) * (g.ny + 2);
-        dim3 grid((unsigned)ceil_div(lines, kZRows), (unsigned)ceil_div(g.nz + 1, 32));
+        dim3 grid((unsigned)ceil_div(lines, kZRows), (unsigned)ceil_div(g.nz + 1, kZOwn));
         if (ctx_.p.geometry)
             k_ctmass_z<true><<<grid, 256, 0, stream_>>>(ctx_);
         else
@@ -872,8 +888,8 @@ void Solver::launch_ctmass()
     } else {
         const int nd = DIR == 0 ? g.nx : g.ny, na = DIR == 0 ? g.ny : g.nx;
         const long long blocks = (long long)(na + 2) * ((g.nz + 1 + ops::kWinK) / ops::kWinK) *
-                                 ((nd + ops::kWinS) / ops::kWinS);
-        const size_t smem = (size_t)ops::SweepCTMass<DIR>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
+                                 ((nd + kCtS) / kCtS);
+        const size_t smem = (size_t)ops::SweepCTMass<DIR>::NARR * kCtP * ops::kWinK * sizeof(double);
         if (ctx_.p.geometry)
             k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_);
         else
