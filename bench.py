@@ -32,18 +32,47 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FP64 cell-updates/s plain vs batched (1 B200, 1e-10 rel); p50/p99 solve latency"
 UNIT = "cell-updates/s"
-# Compulsory FP64 HBM traffic of one resistive cell-update: state read/write
-# per phase, 8 B per value (dt pass 72, predictor 96, corrector 144, three
-# sweeps 3 x 176, two resistive sub-steps 2 x 72).
-ALGO_BYTES_PER_CELL_UPDATE = 984
-def workload(n):
-    return (f"plain LARE3D step, {n}^3 periodic random-field cube [0,1]^3, rho=1, p=0.1, "
-            "|B|rms=0.1, |v|rms=0.05, k=1..8, gamma=5/3, eta=1e-4 (resistive), seeded synthetic IC")
+# Compulsory FP64 HBM traffic of one cell-update: state read/write per
+# phase, 8 B per value (dt pass 72, predictor 96, corrector 144, three sweeps
+# 3 x 176 = 840 B), plus two resistive sub-steps 2 x 72 in resistive runs.
+ALGO_BYTES_IDEAL, ALGO_BYTES_RESISTIVE = 840, 984
 
 
-def l2_note(n):
+class Workload:
+    """One single-solve configuration: case, grid, algorithmic bytes per
+    cell-update and its description (seeded synthetic initial state)."""
+
+    def __init__(self, name, case, grid, algo_bytes, text, tag):
+        self.name, self.case, self.grid, self.algo_bytes, self.text, self.tag = \
+            name, case, tuple(grid), algo_bytes, text, tag
+
+    @property
+    def cells(self):
+        return float(self.grid[0]) * self.grid[1] * self.grid[2]
+
+
+def workload(args):
+    """--config c0 / c1 / c2, or the random-field cube of edge --edge (c1's
+    form; 256 = c1 itself)."""
+    if args.config == "c0":
+        return Workload("c0", "ot", (128, 128, 4), ALGO_BYTES_IDEAL,
+                        "plain LARE3D step, Orszag-Tang 128x128x4 periodic [0,1]^2 x [0,4/128], gamma=5/3, "
+                        "B0=1/sqrt(4 pi), visc1=0.1, visc2=0.5, ideal MHD", "ot128x128x4")
+    if args.config == "c2":
+        return Workload("c2", "harris", (512, 256, 64), ALGO_BYTES_RESISTIVE,
+                        "plain LARE3D step, Harris current sheet 512x256x64 over [-10,10]x[-5,5]x[0,2.5], "
+                        "beta=0.1, 1% seeded velocity perturbation, eta=1e-3, conducting y walls", "harris512x256x64")
+    n = args.edge
+    return Workload("c1" if n == 256 else f"rf{n}", "rf", (n, n, n), ALGO_BYTES_RESISTIVE,
+                    f"plain LARE3D step, {n}^3 periodic random-field cube [0,1]^3, rho=1, p=0.1, "
+                    "|B|rms=0.1, |v|rms=0.05, k=1..8, gamma=5/3, eta=1e-4 (resistive), seeded synthetic IC",
+                    f"rf{n}")
+
+
+def l2_note(w):
     """How the timed inputs relate to the 126 MB L2 of a B200."""
-    field_mb = (n + 5) * (n + 5) * (((n + 6) + 7) // 8 * 8) * 8 / 1e6
+    nx, ny, nz = w.grid
+    field_mb = (nx + 5) * (ny + 5) * (((nz + 6) + 7) // 8 * 8) * 8 / 1e6
     if field_mb * 32 > 126:
         return f"inputs larger than L2 (each field {field_mb:.0f} MB, 32 x {field_mb:.0f} MB resident)"
     return f"inputs fit in L2 (each field {field_mb:.1f} MB): not a full-size run"
@@ -56,6 +85,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sams", choices=["sams", "reference"])
     ap.add_argument("--edge", type=int, default=256, help="cube edge of the plain workload")
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2"],
+                    help="single-solve configuration of the plain line (c1: the 256^3 random-field cube)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -151,10 +182,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(n):
+def ncu_traffic(w):
     """DRAM bytes per step from the committed ncu summary of this workload,
-    if one exists (profiles/lare_step_rf256_traffic.json)."""
-    path = os.path.join(ROOT, "profiles", f"lare_step_rf{n}_traffic.json")
+    if one exists (profiles/lare_step_<tag>_traffic.json)."""
+    path = os.path.join(ROOT, "profiles", f"lare_step_{w.tag}_traffic.json")
     try:
         with open(path) as f:
             return json.load(f)["dram_bytes_per_step"]
@@ -162,13 +193,13 @@ def ncu_traffic(n):
         return None
 
 
-def fp64_roof(n, ms_per_step, rates):
+def fp64_roof(w, ms_per_step, rates):
     """The step's FP64 compute roof: its fp64-pipe warp instructions (ncu
     sm__inst_executed_pipe_fp64 over one step of this workload, committed in
-    profiles/lare_step_rf{n}_fp64.json) at the measured fused multiply-add
+    profiles/lare_step_<tag>_fp64.json) at the measured fused multiply-add
     rate (one warp instruction = 32 thread operations), against the step's
     measured time."""
-    path = os.path.join(ROOT, "profiles", f"lare_step_rf{n}_fp64.json")
+    path = os.path.join(ROOT, "profiles", f"lare_step_{w.tag}_fp64.json")
     try:
         with open(path) as f:
             inst = float(json.load(f)["fp64_pipe_warp_inst_per_step"])
@@ -181,22 +212,23 @@ def fp64_roof(n, ms_per_step, rates):
             "source": os.path.relpath(path, ROOT)}
 
 
-def cpu_reference(n, steps, threads=None):
+def cpu_reference(w, steps, threads=None):
     """Time the reference LARE3D CPU code (or, without its binary, the C
-    restatement) on this host for `steps` steps of the n^3 workload."""
+    restatement) on this host for `steps` steps of workload w."""
     from oracle import lare_oracle as lo
     threads = threads or os.cpu_count()
     env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread")
     binary, isa = lo.reference_bench_binary()
+    nx, ny, nz = w.grid
     if os.path.exists(binary):
-        cmd = [binary, "--case", "rf", "--nx", str(n), "--ny", str(n), "--nz", str(n),
+        cmd = [binary, "--case", w.case, "--nx", str(nx), "--ny", str(ny), "--nz", str(nz),
                "--steps", str(steps), "--seed", "1", "--quiet"]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
         rec = json.loads(out.strip().splitlines()[-1])
         return rec["step_seconds"], "reference", threads, isa
     # the C restatement (ctypes, OpenMP)
-    p, b = lo.case_setup("rf", n, n, n)
-    o = lo.Oracle(p, b, lo.case_fields("rf", p, seed=1))
+    p, b = lo.case_setup(w.case, nx, ny, nz)
+    o = lo.Oracle(p, b, lo.case_fields(w.case, p, seed=1))
     secs = []
     for _ in range(steps):
         t0 = time.perf_counter()
@@ -225,20 +257,21 @@ def replica_throughput(world, cells, steps, ms):
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    n = args.edge
+    w = workload(args)
     total = args.warmup + args.steps
-    secs, kind, threads, isa = cpu_reference(n, total)
+    secs, kind, threads, isa = cpu_reference(w, total)
     timed = secs[args.warmup:]
-    cells = float(n) ** 3
+    cells = w.cells
     value = cells * len(timed) / sum(timed)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": workload(n), "case": "rf", "grid": [n, n, n], "parallelism": "cpu-openmp"},
+        "config": {"workload": w.text, "case": w.case, "grid": list(w.grid), "parallelism": "cpu-openmp"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "isa": isa,
-                         "sample": f"{len(timed)} timed steps of the {n}^3 workload after {args.warmup} warm-up steps"},
+                         "sample": f"{len(timed)} timed steps of the {w.name} workload after {args.warmup} "
+                                   "warm-up steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -249,10 +282,10 @@ def run_sams(args, world, rank, local, pg):
     from sams_b200 import lare
 
     torch.cuda.set_device(local)
-    n = args.edge
-    cells = float(n) ** 3
-    p, b = lare.case_setup("rf", n, n, n)
-    fields = lare.case_fields("rf", p, seed=1 + rank)
+    w = workload(args)
+    cells = w.cells
+    p, b = lare.case_setup(w.case, *w.grid)
+    fields = lare.case_fields(w.case, p, seed=1 + rank)
     # a dedicated stream: the solver launches on it and the events bracket it
     stream = torch.cuda.Stream(device=local)
 
@@ -318,7 +351,7 @@ def run_sams(args, world, rank, local, pg):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
-        box_bytes = int(np.prod(lare.box_shape(n, n, n))) * 8
+        box_bytes = int(np.prod(lare.box_shape(*w.grid))) * 8
         e2e = {"value": replica_throughput(world, cells, args.steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": len(state) * box_bytes / args.steps,
                "d2h_bytes_per_step": (len(state) * box_bytes + 8 * args.steps) / args.steps,
@@ -336,19 +369,19 @@ def run_sams(args, world, rank, local, pg):
     if rank != 0:
         return
     peak, peak_kind = measured_peak()
-    achieved = ALGO_BYTES_PER_CELL_UPDATE * cells / (ms_per_step / 1e3) / 1e9
-    traffic = ncu_traffic(n)
+    achieved = w.algo_bytes * cells / (ms_per_step / 1e3) / 1e9
+    traffic = ncu_traffic(w)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "kernel": "one LARE3D timestep (a CUDA graph of %d kernels)" % launches,
-                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL_UPDATE * cells}
+                "algorithmic_bytes_per_launch": w.algo_bytes * cells}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            csteps = 4 if n >= 256 else 8
-            secs, kind, threads, isa = cpu_reference(n, csteps)
+            csteps = max(4, min(50, int(6.7e7 / cells)))  # about 10 s of host time
+            secs, kind, threads, isa = cpu_reference(w, csteps)
             cpu = {"value": cells * len(secs) / sum(secs), "unit": UNIT, "cores": threads, "kind": kind,
-                   "isa": isa, "sample": f"{csteps} steps of the {n}^3 workload (all steps timed)"}
+                   "isa": isa, "sample": f"{csteps} steps of the {w.name} workload (all steps timed)"}
         except Exception as ex:  # report, do not fail the GPU line
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
@@ -356,16 +389,16 @@ def run_sams(args, world, rank, local, pg):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload(n), "case": "rf", "grid": [n, n, n],
+        "config": {"workload": w.text, "case": w.case, "grid": list(w.grid),
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": l2_note(n)},
+                   "l2": l2_note(w)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": launches * args.steps,
         "batched": batched,
         "served": served,
         "phases_ms": dict(zip(["lagrangian", "corrector", "remap_x", "remap_y", "remap_z"], phases)),
         "fp64_rates_gops": fp64,
-        "fp64_roof": fp64_roof(n, ms_per_step, fp64),
+        "fp64_roof": fp64_roof(w, ms_per_step, fp64),
     }
     print(json.dumps(line), flush=True)
 

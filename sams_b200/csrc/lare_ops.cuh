@@ -704,14 +704,18 @@ struct Pred2 {
                 fy -= rv * uy * ux / r;
             }
         }
-        c.s[S_FX][o] = fx;
-        c.s[S_FY][o] = fy;
-        c.s[S_FZ][o] = fz;
+        // the total force f_visc + f is what both half-steps add (here and in
+        // Corr2, lagran.cpp:757-759): kept as that sum, one array per component
+        const double sx = __ldg(c.s[S_FXV] + o) + fx, sy = __ldg(c.s[S_FYV] + o) + fy,
+                     sz = __ldg(c.s[S_FZV] + o) + fz;
+        c.s[S_FX][o] = sx;
+        c.s[S_FY][o] = sy;
+        c.s[S_FZ][o] = sz;
         const double dt = c.sc->dt;
         const double rho_v = __ldg(c.s[S_RHOV] + o);
-        c.f[SAMS_F_VX1][o] = __ldg(c.f[SAMS_F_VX] + o) + dt / 2.0 * (__ldg(c.s[S_FXV] + o) + fx) / rho_v;
-        c.f[SAMS_F_VY1][o] = __ldg(c.f[SAMS_F_VY] + o) + dt / 2.0 * (__ldg(c.s[S_FYV] + o) + fy) / rho_v;
-        c.f[SAMS_F_VZ1][o] = __ldg(c.f[SAMS_F_VZ] + o) + dt / 2.0 * (__ldg(c.s[S_FZV] + o) + fz) / rho_v;
+        c.f[SAMS_F_VX1][o] = __ldg(c.f[SAMS_F_VX] + o) + dt / 2.0 * sx / rho_v;
+        c.f[SAMS_F_VY1][o] = __ldg(c.f[SAMS_F_VY] + o) + dt / 2.0 * sy / rho_v;
+        c.f[SAMS_F_VZ1][o] = __ldg(c.f[SAMS_F_VZ] + o) + dt / 2.0 * sz / rho_v;
     }
 };
 
@@ -725,6 +729,13 @@ struct Corr1 {
     }
     template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        const Geom &g = c.g;
+        c.s[S_VH][LOFF(i, j, k)] = heating<GEO, P2>(c, i, j, k);
+    }
+    // visc_heat of cell (i, j, k) (the corrector's shock_heating)
+    template <bool GEO, bool P2>
+    __device__ static double heating(const Ctx &c, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
@@ -757,7 +768,7 @@ struct Corr1 {
                      0.25 * dx * dz * a2a[o - SX] * a4 - 0.25 * dy * dz * a1a[o + 1] * a5 - 0.25 * dx * dz * a2a[o + 1] * a6 -
                      0.25 * dy * dz * a1a[o + SY + 1] * a7 - 0.25 * dx * dz * a2a[o - SX + 1] * a8 - 0.25 * dy * dy * a3a[o] * a9 -
                      0.25 * dx * dy * a3a[o - SX] * a10 - 0.25 * dy * dy * a3a[o - SX - SY] * a11 - 0.25 * dx * dy * a3a[o - SY] * a12);
-        c.s[S_VH][o] = pmax(div_by<P2>(vh, cv_at<GEO>(c, i, j, k), c.rc.cv), 0.0);
+        return pmax(div_by<P2>(vh, cv_at<GEO>(c, i, j, k), c.rc.cv), 0.0);
     }
 };
 
@@ -774,16 +785,30 @@ struct Corr2 {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
+        const int o = LOFF(i, j, k);
+        velocity(c, o, c.f[SAMS_F_VX], c.f[SAMS_F_VY], c.f[SAMS_F_VZ]);
+        if (i < 1 || j < 1 || k < 1) return;
+        energy<GEO, P2>(c, i, j, k, __ldg(c.s[S_VH] + o));
+    }
+    // the node's final velocity into nvx/nvy/nvz[o] (the solve's own
+    // arrays in place, or the fused corrector's out-of-place arrays)
+    __device__ static void velocity(const Ctx &c, int o, double *nvx, double *nvy, double *nvz)
+    {
+        const double dt = c.sc->dt;
+        const double rho_v = __ldg(c.s[S_RHOV] + o);
+        const double vxo = c.f[SAMS_F_VX][o], vyo = c.f[SAMS_F_VY][o], vzo = c.f[SAMS_F_VZ][o];
+        // S_FX..S_FZ hold the total force f_visc + f (Pred2)
+        nvx[o] = vxo + dt * __ldg(c.s[S_FX] + o) / rho_v;
+        nvy[o] = vyo + dt * __ldg(c.s[S_FY] + o) / rho_v;
+        nvz[o] = vzo + dt * __ldg(c.s[S_FZ] + o) / rho_v;
+    }
+    // the cell's energies and density with its visc_heat vh (cells 1..n)
+    template <bool GEO, bool P2>
+    __device__ static void energy(const Ctx &c, int i, int j, int k, double vh)
+    {
+        const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
-        {
-            const double rho_v = __ldg(c.s[S_RHOV] + o);
-            double *vx = c.f[SAMS_F_VX], *vy = c.f[SAMS_F_VY], *vz = c.f[SAMS_F_VZ];
-            vx[o] += dt * (__ldg(c.s[S_FXV] + o) + __ldg(c.s[S_FX] + o)) / rho_v;
-            vy[o] += dt * (__ldg(c.s[S_FYV] + o) + __ldg(c.s[S_FY] + o)) / rho_v;
-            vz[o] += dt * (__ldg(c.s[S_FZV] + o) + __ldg(c.s[S_FZ] + o)) / rho_v;
-        }
-        if (i < 1 || j < 1 || k < 1) return;
         const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
         const int a = o, am = o - SX, bm = o - SY, cm = o - 1;
         double vxb = 0.25 * (vx1[a] + vx1[bm] + vx1[cm] + vx1[bm - 1]);
@@ -800,7 +825,7 @@ struct Corr2 {
         double *rho = c.f[SAMS_F_RHO], *ee = c.f[SAMS_F_ENERGY_ELECTRON], *ei = c.f[SAMS_F_ENERGY_ION];
         double r = rho[o];
         ee[o] -= dv * __ldg(c.s[S_PE] + o) / r;
-        ei[o] += (dt * __ldg(c.s[S_VH] + o) - dv * __ldg(c.s[S_PI] + o)) / r;
+        ei[o] += (dt * vh - dv * __ldg(c.s[S_PI] + o)) / r;
         rho[o] = r / (1.0 + dv);
     }
 };
@@ -858,7 +883,7 @@ struct SweepVol {
         set_bounds(lo, hi, -1, g.nx + 2, -1, g.ny + 2, -1, g.nz + 2);
     }
     template <bool GEO, bool P2>
-    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    __device__ static void run(const Ctx &c, int arg, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
@@ -910,7 +935,9 @@ struct SweepVol {
         c.s[S_R_CV2][o] = cv2;
         c.s[S_R_CV1][o] = vol * (1.0 + dv);
         c.s[S_R_DB1][o] = db1;
-        c.s[S_R_RHO1][o] = __ldg(c.f[SAMS_F_RHO] + o);
+        // rho1 = rho before the sweep; arg 1: the sweep runs out of place
+        // (k_psweep) and reads rho itself, which it does not change
+        if (!arg) c.s[S_R_RHO1][o] = __ldg(c.f[SAMS_F_RHO] + o);
         c.f[SAMS_F_DM][o] = 0.0;
     }
 };
@@ -983,43 +1010,72 @@ struct SweepCT {
 
 // Both constrained-transport updates of a sweep (xremap.cpp:87-115,
 // yremap.cpp:97-127, zremap.cpp:103-121), in the reference's order.
+// arg 0: the updates over 0..n.  arg 1 (x sweep, when the solver folds the
+// remap's B scaling in): first B to flux form (BScale's b * area,
+// remap.cpp:46-50) at every box point, then the updates.  arg 2 (z sweep):
+// the updates, then B back from flux form (BScale's b / (area + none_zero),
+// remap.cpp:91-95) over 0..n.  Each value gets the same single multiply or
+// divide as in BScale, so the results are the same bits.
 template <int DIR>
 struct SweepCTUpd {
     static constexpr int kMinBlocks = 4;  // blocks of 256 per SM (register cap), tuned on B200
-    __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
+    __host__ __device__ static void bounds(const Geom &g, int arg, int *lo, int *hi)
     {
-        set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
+        if (arg == 1)
+            set_bounds(lo, hi, -2, g.nx + 2, -2, g.ny + 2, -2, g.nz + 2);
+        else
+            set_bounds(lo, hi, 0, g.nx, 0, g.ny, 0, g.nz);
     }
     template <bool GEO, bool P2>
-    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    __device__ static void run(const Ctx &c, int arg, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const RO f1{c.s[S_R_CT1]}, f2{c.s[S_R_CT2]};
         double *bx = c.f[SAMS_F_BX], *by = c.f[SAMS_F_BY], *bz = c.f[SAMS_F_BZ];
-        const bool xb = i >= 0, xc = i >= 1, yb = j >= 0, yc = j >= 1, zb = k >= 0, zc = k >= 1;
+        double vx = bx[o], vy = by[o], vz = bz[o];
+        bool wx = false, wy = false, wz = false;  // components to store
+        if (arg == 1) {
+            if (j >= -1 && k >= -1) { vx = vx * dxab_at<GEO>(c, i, j, k); wx = true; }
+            if (i >= -1 && k >= -1) { vy = vy * dyab_at<GEO>(c, i, j, k); wy = true; }
+            if (i >= -1 && j >= -1) { vz = vz * dzab_at<GEO>(c, i, j, k); wz = true; }
+        }
+        const bool in = i >= 0 && i <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
+        const bool xb = in, xc = in && i >= 1, yb = in, yc = in && j >= 1, zb = in, zc = in && k >= 1;
         if (DIR == 0) {
-            if (xc && yb && zc) by[o] = by[o] - f1[o] + f1[o - SX];
-            if (xc && yc && zb) bz[o] = bz[o] - f2[o] + f2[o - SX];
+            if (xc && yb && zc) { vy = vy - f1[o] + f1[o - SX]; wy = true; }
+            if (xc && yc && zb) { vz = vz - f2[o] + f2[o - SX]; wz = true; }
             if (xb && yc && zc) {
-                double t = bx[o] + f1[o] - f1[o - SY];
-                bx[o] = t + f2[o] - f2[o - 1];
+                double t = vx + f1[o] - f1[o - SY];
+                vx = t + f2[o] - f2[o - 1];
+                wx = true;
             }
         } else if (DIR == 1) {
-            if (xb && yc && zc) bx[o] = bx[o] - f1[o] + f1[o - SY];
-            if (xc && yc && zb) bz[o] = bz[o] - f2[o] + f2[o - SY];
+            if (xb && yc && zc) { vx = vx - f1[o] + f1[o - SY]; wx = true; }
+            if (xc && yc && zb) { vz = vz - f2[o] + f2[o - SY]; wz = true; }
             if (xc && yb && zc) {
-                double t = by[o] + f1[o] - f1[o - SX];
-                by[o] = t + f2[o] - f2[o - 1];
+                double t = vy + f1[o] - f1[o - SX];
+                vy = t + f2[o] - f2[o - 1];
+                wy = true;
             }
         } else {
-            if (xb && yc && zc) bx[o] = bx[o] - f1[o] + f1[o - 1];
-            if (xc && yb && zc) by[o] = by[o] - f2[o] + f2[o - 1];
+            if (xb && yc && zc) { vx = vx - f1[o] + f1[o - 1]; wx = true; }
+            if (xc && yb && zc) { vy = vy - f2[o] + f2[o - 1]; wy = true; }
             if (xc && yc && zb) {
-                double t = bz[o] + f1[o] - f1[o - SX];
-                bz[o] = t + f2[o] - f2[o - SY];
+                double t = vz + f1[o] - f1[o - SX];
+                vz = t + f2[o] - f2[o - SY];
+                wz = true;
             }
         }
+        if (arg == 2) {  // every point of 0..n meets BScale's conditions
+            vx = vx / (dxab_at<GEO>(c, i, j, k) + NONE_ZERO);
+            vy = vy / (dyab_at<GEO>(c, i, j, k) + NONE_ZERO);
+            vz = vz / (dzab_at<GEO>(c, i, j, k) + NONE_ZERO);
+            wx = wy = wz = true;
+        }
+        if (wx) bx[o] = vx;
+        if (wy) by[o] = vy;
+        if (wz) bz[o] = vz;
     }
 };
 
@@ -1085,8 +1141,10 @@ struct SweepCTMass {
         else if (DIR == 1) { t1 = g.sx; va1 = -1; t2 = 1; va2 = -g.sx; }
         else { t1 = g.sx; va1 = -g.sy; t2 = g.sy; va2 = -g.sx; }
     }
-    template <class A>
-    __device__ static void quot(const Ctx &c, int i, int j, int k, A st)
+    // scale: B is not yet in flux form (the x sweep with the scaling folded
+    // into SweepCTUpd<0>): form BScale's b * area here, the same product
+    template <bool GEO, class A>
+    __device__ static void quot(const Ctx &c, int i, int j, int k, A st, bool scale)
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
@@ -1095,8 +1153,13 @@ struct SweepCTMass {
         const RO db1{c.s[S_R_DB1]};
         const RO b1{c.f[DIR == 0 ? SAMS_F_BY : SAMS_F_BX]}, b2{c.f[DIR == 2 ? SAMS_F_BY : SAMS_F_BZ]};
         const double dba1 = (db1[o] + db1[o + t1]) * 0.5, dba2 = (db1[o] + db1[o + t2]) * 0.5;
-        st.put(F1, b1[o] / dba1);
-        st.put(F2, b2[o] / dba2);
+        double v1 = b1[o], v2 = b2[o];
+        if (DIR == 0 && scale) {  // by and bz at i >= -1, k >= 0: BScale scales both
+            v1 = v1 * dyab_at<GEO>(c, i, j, k);
+            v2 = v2 * dzab_at<GEO>(c, i, j, k);
+        }
+        st.put(F1, v1 / dba1);
+        st.put(F2, v2 / dba2);
         st.put(DB1, dba1);
         st.put(DB2, dba2);
     }

@@ -1,16 +1,24 @@
 // lare_solver.cu -- kernels and step orchestration of one LARE3D solve.
 //
-// One step on the device, in launch order (reference events in brackets):
+// One step on the device, in launch order (reference events in brackets;
+// the standard path: Cartesian or curvilinear, no rke, every dimension at
+// least three cells, every B edge with a condition):
 //   [startOfTimestep -> lagrangian_step, lagran.cpp:95-173]
 //     CellPrep, NodePrep, Alpha, Visc (+ CFL block minima), DtFinalize,
-//     resistive only: 2 x {ResistRK, ResistB, fill B + energies},
-//     Pred1, Pred2, fill v1
+//     resistive only: 2 x {k_resist_march (ResistRK + ResistB), fill B +
+//     energies}, k_pred_march (Pred1 + Pred2), fill v1
 //   [halfTimestep -> corrector_step, lagran.cpp:739-804]
-//     Corr1, Corr2, fill v + energies + density
+//     Corr1, Corr2, fill v + energies + rho
 //   [endOfTimestep -> eulerian_remap, remap.cpp:23-111]
-//     BScale, 3 x {SweepVol, SweepCvc, SweepCT, SweepCTUpd, SweepMass,
-//                  fill dm along the sweep, SweepS6, SweepS7, SweepS8,
-//                  fill the nine state fields}, BUnscale, fill B
+//     x: SweepVol, SweepCvc, k_ctmass (SweepCT + SweepMass), SweepCTUpd
+//        (with B to flux form, BScale), fill dm along x, k_psweep (S6-S8 out
+//        of place) + k_copy_shell, fill the nine state fields
+//     y: the same without the B scaling
+//     z: SweepVol, SweepCvc, k_ctmass_z, SweepCTUpd (with B back from flux
+//        form), fill dm along z, k_zsweep (S6-S8 in place), fill the state
+//        fields but B, fill B
+// Other solves take the separate kernels (BScale, SweepS6/S7/S8, the rke
+// kernels) where a condition above fails.
 // The runner's step++/time += dt (runner.h:573-574) happens in DtFinalize.
 // Nothing is read back to the host inside a step.
 #include "lare_solver.cuh"
@@ -247,7 +255,7 @@ struct CtStore {
 };
 
 template <int DIR, bool GEO>
-__global__ void __launch_bounds__(ops::kWinThreads, 6) k_ctmass(Ctx c)
+__global__ void __launch_bounds__(ops::kWinThreads, 6) k_ctmass(Ctx c, int scale)
 {
     using F = ops::SweepCTMass<DIR>;
     constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
@@ -263,7 +271,8 @@ __global__ void __launch_bounds__(ops::kWinThreads, 6) k_ctmass(Ctx c)
     const bool ct = a <= na && k <= g.nz, mass = k <= g.nz + 1;
     auto at = [&](int s) { return CtStore{csm, s - s0 + 1, kc}; };
     if (ct)
-        for (int s = s0 - 1 + sl; s <= s1 + 2; s += TS) F::quot(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s));
+        for (int s = s0 - 1 + sl; s <= s1 + 2; s += TS)
+            F::template quot<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), scale != 0);
     __syncthreads();
     if (mass)
         for (int s = s0 + sl; s <= s1; s += TS)
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(256, 6) k_ctmass_z(Ctx c)
     if (ct)
         for (int kk = kc; kk < kZSpan; kk += 32) {
             const int k = k0 - 1 + kk;
-            if (k <= g.nz + 2) F::quot(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk});
+            if (k <= g.nz + 2) F::quot<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk}, false);
         }
     __syncthreads();
     for (int kk = kc; kk < kZOwn; kk += 32) {
@@ -496,6 +505,10 @@ FieldList make_list(unsigned mask)
 }
 
 long long ceil_div(long long a, long long b) { return (a + b - 1) / b; }
+
+// Whether n values split into tiles of w lanes keep at least three quarters
+// of the lanes busy (thin grids, e.g. n x n x 4 solves, leave most idle).
+bool lanes_full(long long n, long long w) { return 4 * n >= 3 * w * ceil_div(n, w); }
 
 }  // namespace
 
@@ -791,10 +804,14 @@ void Solver::launch_psweep()
     const int nd = DIR == 0 ? g.nx : g.ny, na = (DIR == 0 ? g.ny : g.nx) + 1;
     const long long blocks = (long long)na * ((g.nz + ops::kWinK) / ops::kWinK) * ((nd + ops::kWinS) / ops::kWinS);
     const size_t smem = (size_t)ops::SweepFused<DIR>::NARR * ops::WinStore::P * ops::kWinK * sizeof(double);
+    // rho1 (rho before the sweep) is rho itself here: the sweep writes the new
+    // rho elsewhere (SweepVol skipped the copy)
+    Ctx cc = ctx_;
+    cc.s[S_R_RHO1] = ctx_.f[SAMS_F_RHO];
     if (ctx_.p.geometry)
-        k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
+        k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
     else
-        k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, w);
+        k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
     const long long shell = BoxShell{{g.nx, g.ny, g.nz}, 1, 0}.count() + BoxShell{{g.nx, g.ny, g.nz}, 0, 0}.count();
     k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(shell, kThreads), 8L * sm_count_), kThreads, 0, stream_>>>(ctx_, w);
     launches_ += 2;
@@ -875,9 +892,17 @@ void Solver::launch_resist(bool last)
 
 // SweepCT + SweepMass of one sweep (k_ctmass / k_ctmass_z).
 template <int DIR>
-void Solver::launch_ctmass()
+void Solver::launch_ctmass(int scale)
 {
     const Geom &g = ctx_.g;
+    // windows over k (x, y: kWinK lanes over 0..nz+1; z: kZOwn own k per
+    // line): on thin grids the separate kernels keep more lanes busy
+    const bool window = DIR == 2 ? lanes_full(g.nz + 1, kZOwn) : lanes_full(g.nz + 2, ops::kWinK);
+    if (!window) {  // (the solver folds the B scaling in only where the x window runs: scale == 0 here)
+        launch<ops::SweepCT<DIR>>(0);
+        launch<ops::SweepMass<DIR>>(0);
+        return;
+    }
     if (DIR == 2) {
         const long long lines = (long long)(g.nx + 2) * (g.ny + 2);
         dim3 grid((unsigned)ceil_div(lines, kZRows), (unsigned)ceil_div(g.nz + 1, kZOwn));
@@ -891,9 +916,9 @@ void Solver::launch_ctmass()
                                  ((nd + kCtS) / kCtS);
         const size_t smem = (size_t)ops::SweepCTMass<DIR>::NARR * kCtP * ops::kWinK * sizeof(double);
         if (ctx_.p.geometry)
-            k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_);
+            k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale);
         else
-            k_ctmass<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_);
+            k_ctmass<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale);
     }
     ++launches_;
 }
@@ -1000,27 +1025,57 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     if (halo_) halo_->reduce_dt(*this);
     k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);
     ++launches_;
+    // the marching kernels tile k by kMK: on thin grids the separate kernels
+    // (one thread per (j, k) of a plane) keep more lanes busy
+    const bool march = lanes_full(ctx_.g.nz + 1, kMK);
     if (resistive) {
         for (int sub = 0; sub < 2; ++sub) {
-            launch_resist(sub == 1);
+            if (march) {
+                launch_resist(sub == 1);
+            } else {
+                launch<ops::ResistRK>(0);
+                launch<ops::ResistB>(sub == 1 ? 1 : 0);
+            }
             bc_fill(FM_BFIELD | FM_ENERGY);
         }
     }
-    launch_pred(resistive);
+    if (march) {
+        launch_pred(resistive);
+    } else {
+        launch<ops::Pred1>(resistive);
+        launch<ops::Pred2>(0);
+    }
     bc_fill(FM_REMAPV);
     mark(1);
     // ---- corrector ----
+    // (Corr1 and Corr2 as one pass, with the velocities written out of place,
+    // was measured slower on B200: Corr2 runs at 6 blocks per SM alone, at
+    // Corr1's 2 when fused.)
     launch<ops::Corr1>(0);
     launch<ops::Corr2>(0);
     bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY);
     mark(2);
     // ---- remap ----
+    // B to and from flux form (BScale) folded into the x and z sweeps' CT
+    // updates when every B edge has a condition that rewrites all its ghost
+    // points from domain values (no SAMS_BC_NONE edge, and at least three
+    // cells in every dimension: with fewer, an edge copy reads ghost planes
+    // it wrote): the z sweep then unscales 0..n only, and the final B fill
+    // sets the ghosts from those values, as it does after BScale's pass over
+    // the whole box.
+    // The x-sweep half of the fold forms b * area inside k_ctmass, so it also
+    // needs that window kernel (not used on thin grids).
+    const bool thick = std::min(ctx_.g.nx, std::min(ctx_.g.ny, ctx_.g.nz)) >= kBcSequentialBelow;
+    bool b_fill_all = thick && lanes_full(ctx_.g.nz + 2, ops::kWinK);
+    for (int f = SAMS_F_BX; f <= SAMS_F_BZ; ++f)
+        for (int d = 0; d < 3; ++d)
+            for (int e = 0; e < 2; ++e) b_fill_all = b_fill_all && bc_.kind[f][d][e] != SAMS_BC_NONE;
     if (p_.rke) launch<ops::RkeZero>(0);
-    launch<ops::BScale>(0);
-    launch<ops::SweepVol<0>>(0);
+    if (!b_fill_all) launch<ops::BScale>(0);
+    launch<ops::SweepVol<0>>(!p_.rke && psweep_ok_ ? 1 : 0);
     launch<ops::SweepCvc>(0);
-    launch_ctmass<0>();
-    launch<ops::SweepCTUpd<0>>(0);
+    launch_ctmass<0>(b_fill_all ? 1 : 0);
+    launch<ops::SweepCTUpd<0>>(b_fill_all ? 1 : 0);
     bc_fill_dim(FM_DM, 0);
     if (!p_.rke && psweep_ok_) {
         launch_psweep<0>();
@@ -1035,9 +1090,9 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     }
     bc_fill(FM_ALL9);
     mark(3);
-    launch<ops::SweepVol<1>>(0);
+    launch<ops::SweepVol<1>>(!p_.rke && psweep_ok_ ? 1 : 0);
     launch<ops::SweepCvc>(0);
-    launch_ctmass<1>();
+    launch_ctmass<1>(0);
     launch<ops::SweepCTUpd<1>>(0);
     bc_fill_dim(FM_DM, 1);
     if (!p_.rke && psweep_ok_) {
@@ -1055,8 +1110,8 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     mark(4);
     launch<ops::SweepVol<2>>(0);
     launch<ops::SweepCvc>(0);
-    launch_ctmass<2>();
-    launch<ops::SweepCTUpd<2>>(0);
+    launch_ctmass<2>(0);
+    launch<ops::SweepCTUpd<2>>(b_fill_all ? 2 : 0);
     bc_fill_dim(FM_DM, 2);
     if (!p_.rke && ctx_.g.nz + 4 <= kZThreads) {
         const Geom &g = ctx_.g;
@@ -1078,8 +1133,8 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         }
         launch<ops::SweepS8<2>>(0);
     }
-    bc_fill(FM_ALL9);
-    launch<ops::BScale>(1);
+    bc_fill(b_fill_all ? FM_ALL9 & ~FM_BFIELD : FM_ALL9);
+    if (!b_fill_all) launch<ops::BScale>(1);
     bc_fill(FM_BFIELD);
     if (p_.rke) launch<ops::RkeEnergy>(0);  // after the remap (shared_data.h:414-417)
     mark(5);

@@ -105,7 +105,7 @@ private:
     template <int DIR> void launch_psweep();
     void launch_pred(int resistive);
     void launch_resist(bool last);
-    template <int DIR> void launch_ctmass();
+    template <int DIR> void launch_ctmass(int scale);
     int setup_psweep();
     int staging(double **out);
     void free_all();

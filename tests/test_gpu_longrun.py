@@ -89,12 +89,8 @@ def test_c0_orszag_tang_200_steps_against_reference_record():
 
 
 def test_c1_random_field_256_cube_500_steps_against_reference_record():
-    if not os.path.exists(lr.path("c1_rf_256cube_s500")):
-        pytest.skip("record not generated")
     _check("c1_rf_256cube_s500", periodic=True)
 
 
 def test_c2_harris_1000_steps_against_reference_record():
-    if not os.path.exists(lr.path("c2_harris_512x256x64_s1000")):
-        pytest.skip("record not generated")
     _check("c2_harris_512x256x64_s1000", periodic=False)

@@ -123,3 +123,17 @@ def test_checker_matches_reference_with_inconsistent_ghosts(tmp_path, oracle_lib
         ref = d.box(f)
         m = ~np.isnan(ref)
         assert np.array_equal(o.field(f)[m], ref[m]), f
+
+
+def test_longrun_records_are_complete():
+    """The long-run records written from the reference (tests/golden/*.longrun.npz)
+    cover every single-solve configuration at its stated step count."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import longrun as lr
+    for name, case, nx, ny, nz, steps, seed in lr.RUNS:
+        meta, fields = lr.load(name)
+        got = (meta["case"], meta["nx"], meta["ny"], meta["nz"], meta["steps"], meta["seed"])
+        assert got == (case, nx, ny, nz, steps, seed)
+        assert len(meta["dts"]) == steps and set(fields) == set(lr.STATE)
+        assert all(len(h) == 64 and len(v) == lr.NSAMPLES for h, _, v in fields.values())
