@@ -126,22 +126,29 @@ struct CellPrep {
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
+        double rho, pe, pi;
+        c.s[S_CS][o] = sound_speed(c, o, rho, pe, pi);
+        if (resistive) {
+            c.s[S_PE][o] = pe;
+            c.s[S_PI][o] = pi;
+        }
+    }
+    // cs of the cell at offset o, with its rho, p_e and p_i
+    __device__ static double sound_speed(const Ctx &c, int o, double &rho, double &pe, double &pi)
+    {
+        const Geom &g = c.g;
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         double bx1 = 0.5 * (bx[o] + bx[o - g.sx]);
         double by1 = 0.5 * (by[o] + by[o - g.sy]);
         double bz1 = 0.5 * (bz[o] + bz[o - 1]);
         const double gm = c.p.gamma;
-        double rho = __ldg(c.f[SAMS_F_RHO] + o);
-        double pe = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
-        double pi = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ION] + o);
+        rho = __ldg(c.f[SAMS_F_RHO] + o);
+        pe = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ELECTRON] + o);
+        pi = (gm - 1.0) * rho * __ldg(c.f[SAMS_F_ENERGY_ION] + o);
         double p = pe + pi;
         double rmin = pmax(rho, NONE_ZERO);
         double b2 = bx1 * bx1 + by1 * by1 + bz1 * bz1;
-        c.s[S_CS][o] = sqrt((gm * p + b2) / rmin);
-        if (resistive) {
-            c.s[S_PE][o] = pe;
-            c.s[S_PI][o] = pi;
-        }
+        return sqrt((gm * p + b2) / rmin);
     }
 };
 
@@ -156,20 +163,35 @@ struct NodePrep {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const RO rho{c.f[SAMS_F_RHO]}, cs{c.s[S_CS]};
+        const ArraySrc src{{c.f[SAMS_F_RHO], c.s[S_CS]}};
+        run_src<GEO, P2>(c, i, j, k, src, LOFF(i, j, k), g.sx, g.sy, 1);
+    }
+    // rho (array 0) and cs (array 1) of the node's eight cells read through
+    // src(array, q), q = q0 + dx*QX + dy*QY + dz*QZ (dx, dy, dz in {0, 1})
+    template <bool GEO, bool P2, class S>
+    __device__ static void run_src(const Ctx &c, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ)
+    {
+        const Geom &g = c.g;
+        struct Arr {
+            const S &s;
+            int a;
+            __device__ double operator[](int q) const { return s(a, q); }
+        };
+        const Arr rho{src, 0}, cs{src, 1};
         const int ip = i + 1, jp = j + 1, kp = k + 1;
         double cv0 = cv_at<GEO>(c, i, j, k), cv1 = cv_at<GEO>(c, ip, j, k), cv2 = cv_at<GEO>(c, i, jp, k), cv3 = cv_at<GEO>(c, ip, jp, k);
         double cv4 = cv_at<GEO>(c, i, j, kp), cv5 = cv_at<GEO>(c, ip, j, kp), cv6 = cv_at<GEO>(c, i, jp, kp), cv7 = cv_at<GEO>(c, ip, jp, kp);
-        int o0 = LOFF(i, j, k), o1 = LOFF(ip, j, k), o2 = LOFF(i, jp, k), o3 = LOFF(ip, jp, k);
-        int o4 = LOFF(i, j, kp), o5 = LOFF(ip, j, kp), o6 = LOFF(i, jp, kp), o7 = LOFF(ip, jp, kp);
+        const int o0 = q0, o1 = q0 + QX, o2 = q0 + QY, o3 = q0 + QX + QY;
+        const int o4 = q0 + QZ, o5 = q0 + QX + QZ, o6 = q0 + QY + QZ, o7 = q0 + QX + QY + QZ;
+        const int on = LOFF(i, j, k);
         double sum_rho_cv = rho[o0] * cv0 + rho[o1] * cv1 + rho[o2] * cv2 + rho[o3] * cv3 +
                             rho[o4] * cv4 + rho[o5] * cv5 + rho[o6] * cv6 + rho[o7] * cv7;
         double sum_cv = cv0 + cv1 + cv2 + cv3 + cv4 + cv5 + cv6 + cv7;
-        c.s[S_RHOV][o0] = div_by<P2>(sum_rho_cv, sum_cv, 0.125 * c.rc.cv);
+        c.s[S_RHOV][on] = div_by<P2>(sum_rho_cv, sum_cv, 0.125 * c.rc.cv);
         double cv_v = 0.125 * sum_cv;
         double sum = cs[o0] * cv0 + cs[o1] * cv1 + cs[o2] * cv2 + cs[o3] * cv3 +
                      cs[o4] * cv4 + cs[o5] * cv5 + cs[o6] * cv6 + cs[o7] * cv7;
-        c.s[S_CSV][o0] = div_by<P2>(0.125 * sum, cv_v, c.rc.cv);
+        c.s[S_CSV][on] = div_by<P2>(0.125 * sum, cv_v, c.rc.cv);
     }
 };
 
@@ -181,15 +203,17 @@ struct Alpha {
     {
         set_bounds(lo, hi, -1, g.nx + 1, -1, g.ny + 2, 0, g.nz + 2);
     }
-    template <bool GEO, bool P2>
-    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    // the edge viscosity of direction E (0 x, 1 y, 2 z) at (i, j, k), where
+    // that direction's range holds the point
+    template <int E, bool GEO, bool P2>
+    __device__ static void edge(const Ctx &c, int i, int j, int k)
     {
         const Geom &g = c.g;
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
         const RO rho_v{c.s[S_RHOV]}, cs_v{c.s[S_CSV]};
         const double dt = c.sc->dt, visc1 = c.p.visc1, v2n = c.p.visc2_norm;
         const int o = LOFF(i, j, k);
-        if (i >= 0 && j >= 0) {  // alpha1: (0..nx+1, 0..ny+2, 0..nz+2)
+        if (E == 0 && i >= 0 && j >= 0) {  // alpha1: (0..nx+1, 0..ny+2, 0..nz+2)
             int o1 = LOFF(i - 1, j - 1, k - 1), o2 = LOFF(i, j - 1, k - 1);
             int o0 = o1 - g.sx, o3 = o2 + g.sx;
             double dx = c.ax.dxb[i + 2], dxp = c.ax.dxb[i + 3], dxm = c.ax.dxb[i + 1];
@@ -197,7 +221,7 @@ struct Alpha {
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A1][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.xb);
         }
-        if (j >= 0 && j <= g.ny + 1) {  // alpha2: (-1..nx+1, 0..ny+1, 0..nz+2)
+        if (E == 1 && j >= 0 && j <= g.ny + 1) {  // alpha2: (-1..nx+1, 0..ny+1, 0..nz+2)
             int o1 = LOFF(i, j - 1, k - 1), o2 = LOFF(i, j, k - 1);
             int o0 = o1 - g.sy, o3 = o2 + g.sy;
             double dx = c.ax.dyb[j + 2], dxp = c.ax.dyb[j + 3], dxm = c.ax.dyb[j + 1];
@@ -209,7 +233,7 @@ struct Alpha {
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A2][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.yb);
         }
-        if (j <= g.ny + 1 && k <= g.nz + 1) {  // alpha3: (-1..nx+1, -1..ny+1, 0..nz+1)
+        if (E == 2 && j <= g.ny + 1 && k <= g.nz + 1) {  // alpha3: (-1..nx+1, -1..ny+1, 0..nz+1)
             int o1 = o - 1, o2 = o;
             int o0 = o1 - 1, o3 = o2 + 1;
             double dx = c.ax.dzb[k + 2], dxp = c.ax.dzb[k + 3], dxm = c.ax.dzb[k + 1];
@@ -221,6 +245,13 @@ struct Alpha {
             double cs_edge = pmin(cs_v[o1], cs_v[o2]);
             c.s[S_A3][o] = edge_viscosity<P2>(dt, visc1, v2n, vx, vy, vz, rho_v, dvdots, dx, dxm, dxp, cs_edge, o0, o1, o2, o3, c.rc.zb);
         }
+    }
+    template <bool GEO, bool P2>
+    __device__ static void run(const Ctx &c, int, int i, int j, int k)
+    {
+        edge<0, GEO, P2>(c, i, j, k);
+        edge<1, GEO, P2>(c, i, j, k);
+        edge<2, GEO, P2>(c, i, j, k);
     }
 };
 
@@ -885,6 +916,12 @@ struct SweepVol {
     template <bool GEO, bool P2>
     __device__ static void run(const Ctx &c, int arg, int i, int j, int k)
     {
+        compute<GEO, P2>(c, arg, i, j, k, true);
+    }
+    // cv1 of the cell (i, j, k); its outputs are stored where `store`
+    template <bool GEO, bool P2>
+    __device__ static double compute(const Ctx &c, int arg, int i, int j, int k, bool store)
+    {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
         const double dt = c.sc->dt;
@@ -932,13 +969,17 @@ struct SweepVol {
             // hzc * dzb (zremap.cpp:79)
             db1 = ((GEO && c.p.geometry) ? c.gf.hzc[h2_index(c, i, j)] * dzb0 : dzb0) + (vzb - vzbm) * dt;
         }
-        c.s[S_R_CV2][o] = cv2;
-        c.s[S_R_CV1][o] = vol * (1.0 + dv);
-        c.s[S_R_DB1][o] = db1;
-        // rho1 = rho before the sweep; arg 1: the sweep runs out of place
-        // (k_psweep) and reads rho itself, which it does not change
-        if (!arg) c.s[S_R_RHO1][o] = __ldg(c.f[SAMS_F_RHO] + o);
-        c.f[SAMS_F_DM][o] = 0.0;
+        const double cv1 = vol * (1.0 + dv);
+        if (store) {
+            c.s[S_R_CV2][o] = cv2;
+            c.s[S_R_CV1][o] = cv1;
+            c.s[S_R_DB1][o] = db1;
+            // rho1 = rho before the sweep; arg 1: the sweep runs out of place
+            // (k_psweep) and reads rho itself, which it does not change
+            if (!arg) c.s[S_R_RHO1][o] = __ldg(c.f[SAMS_F_RHO] + o);
+            c.f[SAMS_F_DM][o] = 0.0;
+        }
+        return cv1;
     }
 };
 
@@ -952,10 +993,18 @@ struct SweepCvc {
     __device__ static void run(const Ctx &c, int, int i, int j, int k)
     {
         const Geom &g = c.g;
-        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const RO cv1{c.s[S_R_CV1]};
-        c.s[S_R_CVC1][o] = 0.125 * (cv1[o] + cv1[o + SX] + cv1[o + SY] + cv1[o + SX + SY] +
-                                    cv1[o + 1] + cv1[o + SX + 1] + cv1[o + SY + 1] + cv1[o + SX + SY + 1]);
+        const ArraySrc src{{c.s[S_R_CV1]}};
+        const int o = LOFF(i, j, k);
+        node(c, o, src, o, g.sx, g.sy, 1);
+    }
+    // cvc1 at the node at offset o from cv1 of its eight cells read through
+    // src(0, q), q = q0 + dx*QX + dy*QY + dz*QZ (dx, dy, dz in {0, 1})
+    template <class S>
+    __device__ static void node(const Ctx &c, int o, const S &src, int q0, int QX, int QY, int QZ)
+    {
+        c.s[S_R_CVC1][o] = 0.125 * (src(0, q0) + src(0, q0 + QX) + src(0, q0 + QY) + src(0, q0 + QX + QY) +
+                                    src(0, q0 + QZ) + src(0, q0 + QX + QZ) + src(0, q0 + QY + QZ) +
+                                    src(0, q0 + QX + QY + QZ));
     }
 };
 

@@ -4,21 +4,22 @@
 // the standard path: Cartesian or curvilinear, no rke, every dimension at
 // least three cells, every B edge with a condition):
 //   [startOfTimestep -> lagrangian_step, lagran.cpp:95-173]
-//     CellPrep, NodePrep, Alpha, Visc (+ CFL block minima), DtFinalize,
-//     resistive only: 2 x {k_resist_march (ResistRK + ResistB), fill B +
-//     energies}, k_pred_march (Pred1 + Pred2), fill v1
+//     k_cellnode_march (CellPrep + NodePrep), Alpha, Visc (+ CFL block
+//     minima), DtFinalize, resistive only: 2 x {k_resist_march (ResistRK +
+//     ResistB), fill B + energies}, k_pred_march (Pred1 + Pred2), fill v1
 //   [halfTimestep -> corrector_step, lagran.cpp:739-804]
 //     Corr1, Corr2, fill v + energies + rho
 //   [endOfTimestep -> eulerian_remap, remap.cpp:23-111]
-//     x: SweepVol, SweepCvc, k_ctmass (SweepCT + SweepMass), SweepCTUpd
-//        (with B to flux form, BScale), fill dm along x, k_psweep (S6-S8 out
-//        of place) + k_copy_shell, fill the nine state fields
+//     x: k_cellnode_march (SweepVol + SweepCvc), k_ctmass (SweepCT +
+//        SweepMass), SweepCTUpd (with B to flux form, BScale), fill dm along
+//        x, k_psweep (S6-S8 out of place), fill the nine state fields
 //     y: the same without the B scaling
-//     z: SweepVol, SweepCvc, k_ctmass_z, SweepCTUpd (with B back from flux
-//        form), fill dm along z, k_zsweep (S6-S8 in place), fill the state
-//        fields but B, fill B
-// Other solves take the separate kernels (BScale, SweepS6/S7/S8, the rke
-// kernels) where a condition above fails.
+//     z: k_cellnode_march (SweepVol + SweepCvc), k_ctmass_z, SweepCTUpd
+//        (with B back from flux form), fill dm along z, k_zsweep (S6-S8 in
+//        place), fill the state fields but B, fill B
+// Other solves take the separate kernels (CellPrep, NodePrep, SweepVol,
+// SweepCvc, BScale, SweepS6/S7/S8, the rke kernels, k_copy_shell) where a
+// condition above fails (thin grids, rke, a field edge without a condition).
 // The runner's step++/time += dt (runner.h:573-574) happens in DtFinalize.
 // Nothing is read back to the host inside a step.
 #include "lare_solver.cuh"
@@ -184,6 +185,95 @@ __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistiv
         // this one read as i-1, which no thread reads after this barrier
     }
 }
+
+// A cell op feeding a node op that reads it at the node's eight cells, in
+// one kernel: the same march as k_pred_march over nodes -1..n+1 of every
+// dimension, with the cell op over cells -1..n+2.  P::produce computes a
+// cell's ring values (P::NR of them) and, where `own`, stores its outputs
+// (each cell is owned by one block: a chunk, row or column holds its own
+// cells and, at the grid's upper end, the +1 halo cell too);
+// P::consume runs the node op from the ring.
+template <class P, bool GEO, bool P2>
+__global__ void __launch_bounds__(kMThreads, P::kMinBlocks) k_cellnode_march(Ctx c, int arg)
+{
+    extern __shared__ double ring[];  // [P::NR][3 planes][kRP]
+    const Geom &g = c.g;
+    const int nkt = (g.nz + 2 + kMK) / kMK, njt = (g.ny + 2 + kMJ) / kMJ;  // tiles over nodes -1..n+1
+    int b = (int)blockIdx.x;
+    const int tk = b % nkt;
+    b /= nkt;
+    const int tj = b % njt;
+    const int i0 = -1 + (b / njt) * kMI, i1 = min(i0 + kMI - 1, g.nx + 1);
+    const int k0 = -1 + tk * kMK, j0 = -1 + tj * kMJ;
+    const int t = (int)threadIdx.x;
+    auto produce = [&](int i) {
+        const int slot = (i + 3) % 3;
+        for (int p = t; p < kRP; p += kMThreads) {
+            const int pj = p / (kMK + 1), pk = p - pj * (kMK + 1);
+            const int j = j0 + pj, k = k0 + pk;
+            if (j > g.ny + 2 || k > g.nz + 2) continue;
+            const bool own = (pj < kMJ || j == g.ny + 2) && (pk < kMK || k == g.nz + 2) && (i <= i1 || i == g.nx + 2);
+            double out[P::NR];
+            P::template produce<GEO, P2>(c, arg, i, j, k, own, out);
+#pragma unroll
+            for (int a = 0; a < P::NR; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
+        }
+    };
+    const int kc = t % (kMK + 1), jc = t / (kMK + 1);
+    const int j = j0 + jc, k = k0 + kc;
+    const bool on = kc < kMK && jc < kMJ && j <= g.ny + 1 && k <= g.nz + 1;
+    const RingSrc src{ring};
+    produce(i0);
+    for (int i = i0; i <= i1; ++i) {
+        produce(i + 1);
+        __syncthreads();  // the ring's planes i and i+1 are complete
+        if (on) {
+            const int s0 = (i + 3) % 3, s1 = (i + 4) % 3;
+            P::template consume<GEO, P2>(c, arg, i, j, k, src, s0 * kRP + jc * (kMK + 1) + kc, (s1 - s0) * kRP,
+                                         kMK + 1, 1);
+        }
+    }
+}
+
+// CellPrep + NodePrep: each cell's rho and sound speed go into the ring for
+// the node averages, so cs never goes to global memory; in resistive runs
+// (arg 1) the cell's step-start p_e, p_i are stored.
+struct PrepMarch {
+    static constexpr int NR = 2, kMinBlocks = 4;  // register cap tuned on B200
+    template <bool GEO, bool P2>
+    __device__ static void produce(const Ctx &c, int resistive, int i, int j, int k, bool own, double *out)
+    {
+        const int o = box_off(c.g, i, j, k);
+        double pe, pi;
+        out[1] = ops::CellPrep::sound_speed(c, o, out[0], pe, pi);
+        if (resistive && own) {
+            c.s[S_PE][o] = pe;
+            c.s[S_PI][o] = pi;
+        }
+    }
+    template <bool GEO, bool P2, class S>
+    __device__ static void consume(const Ctx &c, int, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ)
+    {
+        ops::NodePrep::run_src<GEO, P2>(c, i, j, k, src, q0, QX, QY, QZ);
+    }
+};
+
+// SweepVol + SweepCvc of one sweep: cv1 goes into the ring for the node
+// volumes cvc1.
+template <int DIR>
+struct VolMarch {
+    static constexpr int NR = 1, kMinBlocks = 4;
+    template <bool GEO, bool P2>
+    __device__ static void produce(const Ctx &c, int arg, int i, int j, int k, bool own, double *out)
+    {
+        out[0] = ops::SweepVol<DIR>::template compute<GEO, P2>(c, arg, i, j, k, own);
+    }
+    template <bool GEO, bool P2, class S>
+    __device__ static void consume(const Ctx &c, int, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ)
+    {
+        ops::SweepCvc::node(c, box_off(c.g, i, j, k), src, q0, QX, QY, QZ);
+    }
+};
 
 // One resistive sub-step (ops::ResistRK then ops::ResistB) in one kernel,
 // out of place for B.  A block owns kMK x kMJ points of a y-z plane of the
@@ -812,9 +902,17 @@ void Solver::launch_psweep()
         k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
     else
         k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
-    const long long shell = BoxShell{{g.nx, g.ny, g.nz}, 1, 0}.count() + BoxShell{{g.nx, g.ny, g.nz}, 0, 0}.count();
-    k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(shell, kThreads), 8L * sm_count_), kThreads, 0, stream_>>>(ctx_, w);
-    launches_ += 2;
+    ++launches_;
+    // The points the sweep does not compute are ghost points of each array;
+    // the fill that follows the sweep rewrites all of them from domain values
+    // when every edge of these fields has a condition and every dimension at
+    // least three cells (see enqueue_step).  Otherwise copy them over.
+    if (!ghosts_refilled(FM_DENSITY | FM_ENERGY | FM_VELOCITY)) {
+        const long long shell = BoxShell{{g.nx, g.ny, g.nz}, 1, 0}.count() + BoxShell{{g.nx, g.ny, g.nz}, 0, 0}.count();
+        k_copy_shell<<<(unsigned)std::min<long long>(ceil_div(shell, kThreads), 8L * sm_count_), kThreads, 0,
+                       stream_>>>(ctx_, w);
+        ++launches_;
+    }
     for (int q = 0; q < 6; ++q) std::swap(ctx_.f[kState[q]], ctx_.s[kOut[q]]);
 }
 
@@ -839,6 +937,23 @@ int Solver::setup_psweep()
         if ((rc = check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm), "psweep smem")))
             return rc;
     return SAMS_OK;
+}
+
+// A cell op + node op pair (k_cellnode_march) over the whole box.
+template <class P>
+void Solver::launch_cellnode(int arg)
+{
+    const Geom &g = ctx_.g;
+    const long long blocks =
+        (long long)((g.nz + 2 + kMK) / kMK) * ((g.ny + 2 + kMJ) / kMJ) * ((g.nx + 2 + kMI) / kMI);
+    const size_t smem = (size_t)P::NR * 3 * kRP * sizeof(double);
+    if (ctx_.p.geometry)
+        k_cellnode_march<P, true, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, arg);
+    else if (ctx_.p.pow2)
+        k_cellnode_march<P, false, true><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, arg);
+    else
+        k_cellnode_march<P, false, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, arg);
+    ++launches_;
 }
 
 // Pred1 + Pred2 fused (k_pred_march); the half-step pressures land in the
@@ -939,6 +1054,24 @@ void Solver::launch(int arg)
     ++launches_;
 }
 
+// Whether a boundary fill of the fields in mask rewrites every ghost point
+// from domain values, whatever the ghosts held before: every (dim, edge) of
+// those fields has a condition (none is SAMS_BC_NONE), and every dimension
+// has at least three cells (with fewer, an edge copy reads ghost planes it
+// wrote).  Each condition reads domain planes of its own dimension; the fills
+// run x, then y, then z, so a point that is a ghost in several dimensions
+// ends with the value the last of them computes from the earlier ones.
+bool Solver::ghosts_refilled(unsigned mask) const
+{
+    if (std::min(ctx_.g.nx, std::min(ctx_.g.ny, ctx_.g.nz)) < kBcSequentialBelow) return false;
+    for (int f = 0; f < SAMS_NFIELDS; ++f)
+        if (mask & (1u << f))
+            for (int d = 0; d < 3; ++d)
+                for (int e = 0; e < 2; ++e)
+                    if (bc_.kind[f][d][e] == SAMS_BC_NONE) return false;
+    return true;
+}
+
 bool Solver::all_periodic(unsigned mask) const
 {
     for (int f = 0; f < SAMS_NFIELDS; ++f)
@@ -1005,8 +1138,15 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     };
     mark(0);
     // ---- Lagrangian predictor ----
-    launch<ops::CellPrep>(resistive);
-    launch<ops::NodePrep>(0);
+    // the marching kernels tile k by kMK: on thin grids the separate kernels
+    // (one thread per (j, k) of a plane) keep more lanes busy
+    const bool march = lanes_full(ctx_.g.nz + 1, kMK);
+    if (march) {
+        launch_cellnode<PrepMarch>(resistive);
+    } else {
+        launch<ops::CellPrep>(resistive);
+        launch<ops::NodePrep>(0);
+    }
     launch<ops::Alpha>(0);
     {
         int lo[3], hi[3];
@@ -1025,9 +1165,6 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     if (halo_) halo_->reduce_dt(*this);
     k_dt_finalize<<<1, 1, 0, stream_>>>(sc_, p_.dt_multiplier, resistive);
     ++launches_;
-    // the marching kernels tile k by kMK: on thin grids the separate kernels
-    // (one thread per (j, k) of a plane) keep more lanes busy
-    const bool march = lanes_full(ctx_.g.nz + 1, kMK);
     if (resistive) {
         for (int sub = 0; sub < 2; ++sub) {
             if (march) {
@@ -1057,23 +1194,21 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     mark(2);
     // ---- remap ----
     // B to and from flux form (BScale) folded into the x and z sweeps' CT
-    // updates when every B edge has a condition that rewrites all its ghost
-    // points from domain values (no SAMS_BC_NONE edge, and at least three
-    // cells in every dimension: with fewer, an edge copy reads ghost planes
-    // it wrote): the z sweep then unscales 0..n only, and the final B fill
-    // sets the ghosts from those values, as it does after BScale's pass over
-    // the whole box.
+    // updates when the B fills rewrite every ghost point (ghosts_refilled):
+    // the z sweep then unscales 0..n only, and the final B fill sets the
+    // ghosts from those values, as it does after BScale's pass over the
+    // whole box.
     // The x-sweep half of the fold forms b * area inside k_ctmass, so it also
     // needs that window kernel (not used on thin grids).
-    const bool thick = std::min(ctx_.g.nx, std::min(ctx_.g.ny, ctx_.g.nz)) >= kBcSequentialBelow;
-    bool b_fill_all = thick && lanes_full(ctx_.g.nz + 2, ops::kWinK);
-    for (int f = SAMS_F_BX; f <= SAMS_F_BZ; ++f)
-        for (int d = 0; d < 3; ++d)
-            for (int e = 0; e < 2; ++e) b_fill_all = b_fill_all && bc_.kind[f][d][e] != SAMS_BC_NONE;
+    const bool b_fill_all = ghosts_refilled(FM_BFIELD) && lanes_full(ctx_.g.nz + 2, ops::kWinK);
     if (p_.rke) launch<ops::RkeZero>(0);
     if (!b_fill_all) launch<ops::BScale>(0);
-    launch<ops::SweepVol<0>>(!p_.rke && psweep_ok_ ? 1 : 0);
-    launch<ops::SweepCvc>(0);
+    if (march) {
+        launch_cellnode<VolMarch<0>>(!p_.rke && psweep_ok_ ? 1 : 0);
+    } else {
+        launch<ops::SweepVol<0>>(!p_.rke && psweep_ok_ ? 1 : 0);
+        launch<ops::SweepCvc>(0);
+    }
     launch_ctmass<0>(b_fill_all ? 1 : 0);
     launch<ops::SweepCTUpd<0>>(b_fill_all ? 1 : 0);
     bc_fill_dim(FM_DM, 0);
@@ -1090,8 +1225,12 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     }
     bc_fill(FM_ALL9);
     mark(3);
-    launch<ops::SweepVol<1>>(!p_.rke && psweep_ok_ ? 1 : 0);
-    launch<ops::SweepCvc>(0);
+    if (march) {
+        launch_cellnode<VolMarch<1>>(!p_.rke && psweep_ok_ ? 1 : 0);
+    } else {
+        launch<ops::SweepVol<1>>(!p_.rke && psweep_ok_ ? 1 : 0);
+        launch<ops::SweepCvc>(0);
+    }
     launch_ctmass<1>(0);
     launch<ops::SweepCTUpd<1>>(0);
     bc_fill_dim(FM_DM, 1);
@@ -1108,8 +1247,12 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     }
     bc_fill(FM_ALL9);
     mark(4);
-    launch<ops::SweepVol<2>>(0);
-    launch<ops::SweepCvc>(0);
+    if (march) {
+        launch_cellnode<VolMarch<2>>(0);
+    } else {
+        launch<ops::SweepVol<2>>(0);
+        launch<ops::SweepCvc>(0);
+    }
     launch_ctmass<2>(0);
     launch<ops::SweepCTUpd<2>>(b_fill_all ? 2 : 0);
     bc_fill_dim(FM_DM, 2);

@@ -101,8 +101,10 @@ private:
     void bc_fill(unsigned mask);
     void bc_fill_dim(unsigned mask, int dim);
     bool all_periodic(unsigned mask) const;
+    bool ghosts_refilled(unsigned mask) const;
     template <class Op> void launch(int arg);
     template <int DIR> void launch_psweep();
+    template <class P> void launch_cellnode(int arg);
     void launch_pred(int resistive);
     void launch_resist(bool last);
     template <int DIR> void launch_ctmass(int scale);
