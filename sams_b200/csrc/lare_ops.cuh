@@ -764,31 +764,74 @@ struct Corr1 {
         const Geom &g = c.g;
         c.s[S_VH][LOFF(i, j, k)] = heating<GEO, P2>(c, i, j, k);
     }
+    // Product of the velocity jumps at the start of the step and of the
+    // half step along an edge.  Swapping a and b negates both factors, which
+    // gives the same product up to the sign of a zero; a cell's heating is
+    // clamped at +0.0, so the sign of a zero never shows.
+    __device__ __forceinline__ static double dd(const Ctx &c, int a, int b)
+    {
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
+        const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
+        return 1 * ((vx[a] - vx[b]) * (vx1[a] - vx1[b]) + (vy[a] - vy[b]) * (vy1[a] - vy1[b]) +
+                    (vz[a] - vz[b]) * (vz1[a] - vz1[b]));
+    }
+    // The products of the x, y and z edges that end at node o, formed once
+    // per node by the marching kernel (k_edge_march).
+    __device__ __forceinline__ static void node_edges(const Ctx &c, int o, double *e)
+    {
+        e[0] = dd(c, o - c.g.sx, o);
+        e[1] = dd(c, o - c.g.sy, o);
+        e[2] = dd(c, o - 1, o);
+    }
+    // a1..a12 of cell (i, j, k) from the marching kernel's ring (q0: node
+    // (i, j, k)).  The shock heating's x and y edges are at k and k+1 and
+    // its z edges end at k (lagran.cpp:888-979).
+    template <class S>
+    __device__ __forceinline__ static void ring_edges(const S &src, int q0, int QX, int QY, double *a)
+    {
+        a[0] = src(0, q0 - QY);
+        a[1] = src(1, q0);
+        a[2] = src(0, q0);
+        a[3] = src(1, q0 - QX);
+        a[4] = src(0, q0 - QY + 1);
+        a[5] = src(1, q0 + 1);
+        a[6] = src(0, q0 + 1);
+        a[7] = src(1, q0 - QX + 1);
+        a[8] = src(2, q0);
+        a[9] = src(2, q0 - QX);
+        a[10] = src(2, q0 - QX - QY);
+        a[11] = src(2, q0 - QY);
+    }
     // visc_heat of cell (i, j, k) (the corrector's shock_heating)
     template <bool GEO, bool P2>
     __device__ static double heating(const Ctx &c, int i, int j, int k)
     {
         const Geom &g = c.g;
         const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
-        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
-        const RO vx1{c.f[SAMS_F_VX1]}, vy1{c.f[SAMS_F_VY1]}, vz1{c.f[SAMS_F_VZ1]};
-        const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
-#define DD(a, b) (1 * ((vx[a] - vx[b]) * (vx1[a] - vx1[b]) + (vy[a] - vy[b]) * (vy1[a] - vy1[b]) + \
-                       (vz[a] - vz[b]) * (vz1[a] - vz1[b])))
         const int mm0 = o - SX - SY, m00 = o - SX, om0 = o - SY;
-        double a1 = DD(mm0, om0);
-        double a2 = DD(om0, o);
-        double a3 = DD(o, m00);
-        double a4 = DD(m00, mm0);
-        double a5 = DD(mm0 + 1, om0 + 1);
-        double a6 = DD(om0 + 1, o + 1);
-        double a7 = DD(o + 1, m00 + 1);
-        double a8 = DD(m00 + 1, mm0 + 1);
-        double a9 = DD(o - 1, o);
-        double a10 = DD(m00 - 1, m00);
-        double a11 = DD(mm0 - 1, mm0);
-        double a12 = DD(om0 - 1, om0);
-#undef DD
+        double a[12];
+        a[0] = dd(c, mm0, om0);
+        a[1] = dd(c, om0, o);
+        a[2] = dd(c, o, m00);
+        a[3] = dd(c, m00, mm0);
+        a[4] = dd(c, mm0 + 1, om0 + 1);
+        a[5] = dd(c, om0 + 1, o + 1);
+        a[6] = dd(c, o + 1, m00 + 1);
+        a[7] = dd(c, m00 + 1, mm0 + 1);
+        a[8] = dd(c, o - 1, o);
+        a[9] = dd(c, m00 - 1, m00);
+        a[10] = dd(c, mm0 - 1, mm0);
+        a[11] = dd(c, om0 - 1, om0);
+        return heating_finish<GEO, P2>(c, i, j, k, a);
+    }
+    template <bool GEO, bool P2>
+    __device__ __forceinline__ static double heating_finish(const Ctx &c, int i, int j, int k, const double *a)
+    {
+        const Geom &g = c.g;
+        const int SX = g.sx, SY = g.sy, o = LOFF(i, j, k);
+        const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
+        const double a1 = a[0], a2 = a[1], a3 = a[2], a4 = a[3], a5 = a[4], a6 = a[5];
+        const double a7 = a[6], a8 = a[7], a9 = a[8], a10 = a[9], a11 = a[10], a12 = a[11];
         const double dx = c.ax.dxb[i + 2];
         double dy = c.ax.dyb[j + 2], dz = c.ax.dzb[k + 2];
         if (GEO && c.p.geometry) {  // lagran.cpp:980-982

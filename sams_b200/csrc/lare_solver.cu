@@ -8,7 +8,8 @@
 //     minima), DtFinalize, resistive only: 2 x {k_resist_march (ResistRK +
 //     ResistB), fill B + energies}, k_pred_march (Pred1 + Pred2), fill v1
 //   [halfTimestep -> corrector_step, lagran.cpp:739-804]
-//     Corr1, Corr2, fill v + energies + rho
+//     k_edge_march (Corr1 from per-node edge terms), Corr2, fill v +
+//     energies + rho
 //   [endOfTimestep -> eulerian_remap, remap.cpp:23-111]
 //     x: k_cellnode_march (SweepVol + SweepCvc), k_ctmass (SweepCT +
 //        SweepMass), SweepCTUpd (with B to flux form, BScale), fill dm along
@@ -17,8 +18,8 @@
 //     z: k_cellnode_march (SweepVol + SweepCvc), k_ctmass_z, SweepCTUpd
 //        (with B back from flux form), fill dm along z, k_zsweep (S6-S8 in
 //        place), fill the state fields but B, fill B
-// Other solves take the separate kernels (CellPrep, NodePrep, SweepVol,
-// SweepCvc, BScale, SweepS6/S7/S8, the rke kernels, k_copy_shell) where a
+// Other solves take the separate kernels (CellPrep, NodePrep, Corr1,
+// SweepVol, SweepCvc, BScale, SweepS6/S7/S8, the rke kernels, k_copy_shell) where a
 // condition above fails (thin grids, rke, a field edge without a condition).
 // The runner's step++/time += dt (runner.h:573-574) happens in DtFinalize.
 // Nothing is read back to the host inside a step.
@@ -272,6 +273,75 @@ struct VolMarch {
     __device__ static void consume(const Ctx &c, int, int i, int j, int k, const S &src, int q0, int QX, int QY, int QZ)
     {
         ops::SweepCvc::node(c, box_off(c.g, i, j, k), src, q0, QX, QY, QZ);
+    }
+};
+
+// An edge term feeding a cell op that reads it on twelve edges around the
+// cell, in one kernel (used for the shock heating, whose twelve products of
+// velocity jumps per cell, lagran.cpp:888-979, are terms of the edges
+// between the cell's corner nodes).  Each term is formed once, at the node
+// where its edge ends, instead of once for each of the four cells that share
+// the edge.  The march of k_pred_march over cells 0..n+1: for each plane i
+// the block forms the x, y and z edge terms of the nodes of plane i that its
+// cells read (rows j0-1 .. j0+kMJ-1, kMK+1 columns from k0 + P::KOFF) into a
+// ring of three planes in shared memory, then runs the cell op for its cells
+// of plane i from the ring's planes i-1 and i.
+template <class P, bool GEO, bool P2>
+__global__ void __launch_bounds__(kMThreads, (P2 ? P::kMinBlocksP2 : P::kMinBlocks)) k_edge_march(Ctx c)
+{
+    extern __shared__ double ring[];  // [3 edge directions][3 planes][kRP]
+    const Geom &g = c.g;
+    const int nkt = (g.nz + 1 + kMK) / kMK, njt = (g.ny + 1 + kMJ) / kMJ;  // tiles over cells 0..n+1
+    int b = (int)blockIdx.x;
+    const int tk = b % nkt;
+    b /= nkt;
+    const int tj = b % njt;
+    const int i0 = (b / njt) * kMI, i1 = min(i0 + kMI - 1, g.nx + 1);
+    const int k0 = tk * kMK, j0 = tj * kMJ;
+    const int t = (int)threadIdx.x;
+    const int kmax = g.nz + 2 + P::KOFF;  // last node column the cells read
+    auto produce = [&](int i) {
+        const int slot = (i + 3) % 3;
+        for (int p = t; p < kRP; p += kMThreads) {
+            const int pj = p / (kMK + 1), pk = p - pj * (kMK + 1);
+            const int j = j0 - 1 + pj, k = k0 + P::KOFF + pk;
+            if (j > g.ny + 1 || k > kmax) continue;
+            double e[3];
+            P::Op::node_edges(c, box_off(g, i, j, k), e);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) ring[(a * 3 + slot) * kRP + p] = e[a];
+        }
+    };
+    const int kc = t % (kMK + 1), jc = t / (kMK + 1);
+    const int j = j0 + jc, k = k0 + kc;
+    const bool on = kc < kMK && jc < kMJ && j <= g.ny + 1 && k <= g.nz + 1;
+    const RingSrc src{ring};
+    produce(i0 - 1);
+    for (int i = i0; i <= i1; ++i) {
+        produce(i);
+        __syncthreads();  // the ring's planes i-1 and i are complete
+        if (on) {
+            const int s0 = (i + 3) % 3, sm = (i + 2) % 3;
+            double a[12];
+            P::Op::ring_edges(src, s0 * kRP + (jc + 1) * (kMK + 1) + (kc - P::KOFF), (s0 - sm) * kRP, kMK + 1, a);
+            P::template finish<GEO, P2>(c, i, j, k, a);
+        }
+        // three ring planes: the next iteration's producer writes the plane
+        // this one read as i-2, which no thread reads any more
+    }
+}
+
+// Corr1 from the ring of products of velocity jumps: the shock heating.
+// (Corr2's energy and density update folded in here, with only its velocity
+// update left as a kernel, measured slower on B200: 0.83 + 0.25 ms against
+// 0.43 + 0.60.)
+struct HeatEdges {
+    using Op = ops::Corr1;
+    static constexpr int KOFF = 0, kMinBlocks = 4, kMinBlocksP2 = 4;  // register cap tuned on B200
+    template <bool GEO, bool P2>
+    __device__ static void finish(const Ctx &c, int i, int j, int k, const double *a)
+    {
+        c.s[S_VH][box_off(c.g, i, j, k)] = Op::heating_finish<GEO, P2>(c, i, j, k, a);
     }
 };
 
@@ -532,30 +602,32 @@ __global__ void __launch_bounds__(kThreads) k_bc_periodic(Ctx c, FieldList fl)
         ext[d] = n[d] + 3 - lb[d];
         gh[d] = ext[d] - n[d];
     }
-    const long long A = (long long)gh[0] * ext[1] * ext[2];
-    const long long B = (long long)n[0] * gh[1] * ext[2];
-    const long long C = (long long)n[0] * n[1] * gh[2];
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    // 32-bit index arithmetic: a field's shell has fewer points than the
+    // field, and a field has fewer than 2^31 (checked at set-up)
+    const int A = gh[0] * ext[1] * ext[2];
+    const int B = n[0] * gh[1] * ext[2];
+    const int C = n[0] * n[1] * gh[2];
+    int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     int q[3];
     if (t < A) {
-        int gi = (int)(t / ((long long)ext[1] * ext[2]));
-        long long r = t % ((long long)ext[1] * ext[2]);
+        const int pl = ext[1] * ext[2];
+        const int gi = t / pl, r = t - gi * pl;
         q[0] = gi < 1 - lb[0] ? lb[0] + gi : n[0] + 1 + (gi - (1 - lb[0]));
-        q[1] = lb[1] + (int)(r / ext[2]);
-        q[2] = lb[2] + (int)(r % ext[2]);
+        q[1] = lb[1] + r / ext[2];
+        q[2] = lb[2] + r % ext[2];
     } else if ((t -= A) < B) {
-        int i = (int)(t / ((long long)gh[1] * ext[2]));
-        long long r = t % ((long long)gh[1] * ext[2]);
-        int gj = (int)(r / ext[2]);
+        const int pl = gh[1] * ext[2];
+        const int i = t / pl, r = t - i * pl;
+        const int gj = r / ext[2];
         q[0] = 1 + i;
         q[1] = gj < 1 - lb[1] ? lb[1] + gj : n[1] + 1 + (gj - (1 - lb[1]));
-        q[2] = lb[2] + (int)(r % ext[2]);
+        q[2] = lb[2] + (r - gj * ext[2]);
     } else if ((t -= B) < C) {
-        int i = (int)(t / ((long long)n[1] * gh[2]));
-        long long r = t % ((long long)n[1] * gh[2]);
-        int gk = (int)(r % gh[2]);
+        const int pl = n[1] * gh[2];
+        const int i = t / pl, r = t - i * pl;
+        const int gk = r % gh[2];
         q[0] = 1 + i;
-        q[1] = 1 + (int)(r / gh[2]);
+        q[1] = 1 + r / gh[2];
         q[2] = gk < 1 - lb[2] ? lb[2] + gk : n[2] + 1 + (gk - (1 - lb[2]));
     } else {
         return;
@@ -956,6 +1028,23 @@ void Solver::launch_cellnode(int arg)
     ++launches_;
 }
 
+// A marching edge-term kernel (k_edge_march) over cells 0..n+1.
+template <class P>
+void Solver::launch_edges()
+{
+    const Geom &g = ctx_.g;
+    const long long blocks =
+        (long long)((g.nz + 1 + kMK) / kMK) * ((g.ny + 1 + kMJ) / kMJ) * ((g.nx + 1 + kMI) / kMI);
+    const size_t smem = (size_t)3 * 3 * kRP * sizeof(double);
+    if (ctx_.p.geometry)
+        k_edge_march<P, true, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_);
+    else if (ctx_.p.pow2)
+        k_edge_march<P, false, true><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_);
+    else
+        k_edge_march<P, false, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_);
+    ++launches_;
+}
+
 // Pred1 + Pred2 fused (k_pred_march); the half-step pressures land in the
 // S_CS / S_CSV arrays (free from here to the remap), whose slots then swap
 // with S_PE / S_PI.
@@ -1188,7 +1277,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     // (Corr1 and Corr2 as one pass, with the velocities written out of place,
     // was measured slower on B200: Corr2 runs at 6 blocks per SM alone, at
     // Corr1's 2 when fused.)
-    launch<ops::Corr1>(0);
+    if (march)
+        launch_edges<HeatEdges>();
+    else
+        launch<ops::Corr1>(0);
     launch<ops::Corr2>(0);
     bc_fill(FM_VELOCITY | FM_ENERGY | FM_DENSITY);
     mark(2);

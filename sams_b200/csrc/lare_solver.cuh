@@ -105,6 +105,7 @@ private:
     template <class Op> void launch(int arg);
     template <int DIR> void launch_psweep();
     template <class P> void launch_cellnode(int arg);
+    template <class P> void launch_edges();
     void launch_pred(int resistive);
     void launch_resist(bool last);
     template <int DIR> void launch_ctmass(int scale);
