@@ -14,10 +14,11 @@
 //     x: k_cellnode_march (SweepVol + SweepCvc), k_ctmass (SweepCT +
 //        SweepMass), SweepCTUpd (with B to flux form, BScale), fill dm along
 //        x, k_psweep (S6-S8 out of place), fill the nine state fields
-//     y: the same without the B scaling
-//     z: k_cellnode_march (SweepVol + SweepCvc), k_ctmass_z, SweepCTUpd
-//        (with B back from flux form), fill dm along z, k_zsweep (S6-S8 in
-//        place), fill the state fields but B, fill B
+//     y: k_cellnode_march, k_ctmass, fill dm along y, k_psweep (S6-S8 out
+//        of place, with SweepCTUpd), fill the nine state fields
+//     z: k_cellnode_march (SweepVol + SweepCvc), k_ctmass_z, fill dm along
+//        z, k_zsweep (S6-S8 in place, with SweepCTUpd bringing B back from
+//        flux form), fill the state fields but B, fill B
 // Other solves take the separate kernels (CellPrep, NodePrep, Corr1,
 // SweepVol, SweepCvc, BScale, SweepS6/S7/S8, the rke kernels, k_copy_shell) where a
 // condition above fails (thin grids, rke, a field edge without a condition).
@@ -60,8 +61,11 @@ __global__ void __launch_bounds__(kThreads, (MinBlocks<Op, P2>::value)) k_op(Ctx
 // 0..ny, one thread per k = -2..nz+1 of each.
 constexpr int kZThreads = ops::kZLineThreads;
 
+// ct_arg >= 0: each point of 0..n also takes the z sweep's CT update of B
+// (SweepCTUpd<2> with that argument), which nothing else in the kernel reads
+// or writes.
 template <bool GEO>
-__global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per SM, tuned on B200
+__global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c, int ct_arg)  // 4 blocks per SM, tuned on B200
 {
     using F = ops::SweepFused<2>;
     extern __shared__ double zsm[];
@@ -78,6 +82,7 @@ __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per
     if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st, w, true);
     __syncthreads();
     if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st, w);
+    if (ct_arg >= 0 && on && k >= 0 && k <= g.nz) ops::SweepCTUpd<2>::run<GEO, false>(c, ct_arg, i, j, k);
 }
 
 // The x or y sweep's stages (ops::SweepFused<DIR>) out of place, over
@@ -85,9 +90,11 @@ __global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c)  // 4 blocks per
 // one value of the third index (j for x, i for y) in 0..n.  The solve's
 // state arrays are only read; the new rho, energies and velocities go to w.
 // Halo points recompute stage A (two before, one after) and stage B (one
-// before) without writing the state.
+// before) without writing the state.  ct_arg >= 0: each own point (0..n in
+// every dimension) also takes the sweep's CT update of B (SweepCTUpd<DIR>
+// with that argument); no stage reads B.
 template <int DIR, bool GEO>
-__global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::SweepOut w)  // window shape and cap tuned on B200
+__global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::SweepOut w, int ct_arg)  // window shape and cap tuned on B200
 {
     using F = ops::SweepFused<DIR>;
     constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
@@ -112,6 +119,9 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::Swee
     __syncthreads();
     for (int s = s0 + sl; s <= s1; s += TS)
         if (on) F::stage_c(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w);
+    if (ct_arg >= 0)
+        for (int s = s0 + sl; s <= s1; s += TS)
+            if (on) ops::SweepCTUpd<DIR>::template run<GEO, false>(c, ct_arg, DIR == 0 ? s : a, DIR == 0 ? a : s, k);
 }
 
 // The predictor (ops::Pred1 then ops::Pred2) in one kernel.  A block owns
@@ -955,7 +965,7 @@ int Solver::download(int field, double *dst, cudaMemcpyKind kind)
 // the arrays the x sweep left, so after the two sweeps every pointer is
 // where it started.
 template <int DIR>
-void Solver::launch_psweep()
+void Solver::launch_psweep(int ct_arg)
 {
     static const int kOut[6] = {S_FX, S_FY, S_FZ, S_VH, S_FXV, S_FYV};
     static const int kState[6] = {SAMS_F_RHO, SAMS_F_ENERGY_ELECTRON, SAMS_F_ENERGY_ION,
@@ -971,9 +981,9 @@ void Solver::launch_psweep()
     Ctx cc = ctx_;
     cc.s[S_R_RHO1] = ctx_.f[SAMS_F_RHO];
     if (ctx_.p.geometry)
-        k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
+        k_psweep<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w, ct_arg);
     else
-        k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w);
+        k_psweep<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(cc, w, ct_arg);
     ++launches_;
     // The points the sweep does not compute are ghost points of each array;
     // the fill that follows the sweep rewrites all of them from domain values
@@ -1302,10 +1312,17 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepCvc>(0);
     }
     launch_ctmass<0>(b_fill_all ? 1 : 0);
+    // The CT update changes only B, which the dm fill and the stages S6-S8
+    // do not read, so the y and z sweeps' fused stages take it at their
+    // points 0..n (its whole range).  In the x sweep, with the B scaling
+    // folded in, it stays a kernel of its own: inside k_psweep it measured
+    // slower on B200 (14 us per step), in the y and z sweeps faster (13 and
+    // 40 us).
+    const bool fused_xy = !p_.rke && psweep_ok_;  // k_psweep runs the x and y stages
     launch<ops::SweepCTUpd<0>>(b_fill_all ? 1 : 0);
     bc_fill_dim(FM_DM, 0);
-    if (!p_.rke && psweep_ok_) {
-        launch_psweep<0>();
+    if (fused_xy) {
+        launch_psweep<0>(-1);
     } else {
         launch<ops::SweepS6<0>>(0);
         launch<ops::SweepS7<0>>(0);
@@ -1324,10 +1341,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepCvc>(0);
     }
     launch_ctmass<1>(0);
-    launch<ops::SweepCTUpd<1>>(0);
+    if (!fused_xy) launch<ops::SweepCTUpd<1>>(0);
     bc_fill_dim(FM_DM, 1);
-    if (!p_.rke && psweep_ok_) {
-        launch_psweep<1>();
+    if (fused_xy) {
+        launch_psweep<1>(0);
     } else {
         launch<ops::SweepS6<1>>(0);
         launch<ops::SweepS7<1>>(0);
@@ -1346,18 +1363,20 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepCvc>(0);
     }
     launch_ctmass<2>(0);
-    launch<ops::SweepCTUpd<2>>(b_fill_all ? 2 : 0);
+    const bool zfused = !p_.rke && ctx_.g.nz + 4 <= kZThreads;
+    if (!zfused) launch<ops::SweepCTUpd<2>>(b_fill_all ? 2 : 0);
     bc_fill_dim(FM_DM, 2);
-    if (!p_.rke && ctx_.g.nz + 4 <= kZThreads) {
+    if (zfused) {
         const Geom &g = ctx_.g;
         const int W = g.nz + 4, lines = kZThreads / W;
         const long long nl = (long long)(g.nx + 1) * (g.ny + 1);
         const size_t smem = (size_t)ops::SweepFused<2>::NARR * lines * W * sizeof(double);
         const unsigned blocks = (unsigned)ceil_div(nl, lines);
+        const int ct_arg = b_fill_all ? 2 : 0;
         if (ctx_.p.geometry)
-            k_zsweep<true><<<blocks, kZThreads, smem, stream_>>>(ctx_);
+            k_zsweep<true><<<blocks, kZThreads, smem, stream_>>>(ctx_, ct_arg);
         else
-            k_zsweep<false><<<blocks, kZThreads, smem, stream_>>>(ctx_);
+            k_zsweep<false><<<blocks, kZThreads, smem, stream_>>>(ctx_, ct_arg);
         ++launches_;
     } else {
         launch<ops::SweepS6<2>>(0);

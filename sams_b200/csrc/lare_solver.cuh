@@ -103,7 +103,7 @@ private:
     bool all_periodic(unsigned mask) const;
     bool ghosts_refilled(unsigned mask) const;
     template <class Op> void launch(int arg);
-    template <int DIR> void launch_psweep();
+    template <int DIR> void launch_psweep(int ct_arg);
     template <class P> void launch_cellnode(int arg);
     template <class P> void launch_edges();
     void launch_pred(int resistive);
