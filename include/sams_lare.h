@@ -175,11 +175,15 @@ int sams_lare_batch_autotune(sams_lare_batch *b, int trial_steps, int *tile_plan
 int sams_lare_batch_device_bytes(sams_lare_batch *b, int64_t *bytes);
 
 /* ---- Serving: continuous batching under a device-memory budget ----------
- * A scheduler thread keeps a batch of running solves resident on the GPU and
- * advances them together one step at a time; queued requests are admitted in
- * arrival order as soon as their device footprint fits the budget, and each
- * finished solve's state is copied to the host and its memory freed.  The
- * reference has no serving layer (one runner = one solve, runner.h:564-586). */
+ * A scheduler thread keeps the running solves resident on the GPU and
+ * advances them together one step at a time: solves whose z lines fill the
+ * single-solve path's fused kernels each launch their own step graph on their
+ * own stream, the rest share one batched step, and all of these overlap on
+ * the device.  Queued requests are admitted in arrival order as soon as
+ * their device footprint fits the budget, and each finished solve's state is
+ * copied to the host and its memory freed.  A solve's result is the same
+ * bits on either path.  The reference has no serving layer (one runner = one
+ * solve, runner.h:564-586). */
 typedef struct sams_lare_server sams_lare_server;
 
 enum sams_serve_status {

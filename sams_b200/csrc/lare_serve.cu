@@ -6,16 +6,23 @@
 //   1. admit queued requests in arrival order while their device footprint
 //      fits the budget and, when a cap is set, the interior cells of the
 //      running solves stay under it (allocate, upload the initial state);
-//   2. advance every running solve together by one batched step (one graph
-//      launch; the graph is re-recorded when the running set changes);
+//   2. advance every running solve by one step: solves whose step runs the
+//      single-solve path's fused kernels (Solver::fused_path: z lines long
+//      enough to fill their tiles) each launch their own step graph on their
+//      own stream, and all other solves advance together by one batched
+//      step (one graph launch; re-recorded when that set changes), on one
+//      more stream, so the steps of all running solves overlap on the GPU;
 //   3. retire solves that reached their step count: copy the state to the
 //      host, free the device memory, stamp the completion time.
+// Either path gives a solve the same bits (both equal the reference's), so
+// where a solve runs changes its speed, not its result.
 // State stays resident on the device from admission to retirement, and a
 // request that arrives while others run is admitted as soon as memory frees
 // up, so its steps overlap theirs on the device.  A solve whose CFL timestep
 // goes non-finite is retired as failed without stopping the others.
 #include "sams_lare.h"
 #include "lare_batch.cuh"
+#include "lare_solver.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -44,7 +51,9 @@ struct Request {
     int64_t nsteps = 0;
     int64_t done = 0;
     long long cells = 0;
-    int slot = -1;
+    int slot = -1;                          // batch slot (batched solves)
+    std::unique_ptr<sams::Solver> solo;     // own solver (fused-path solves)
+    bool fused = false;
     int status = SAMS_SERVE_QUEUED;
     bool cancel = false;  // set by sams_lare_serve_cancel while running
     long long bytes = 0;
@@ -58,6 +67,7 @@ const int kStateFields[9] = {SAMS_F_RHO, SAMS_F_ENERGY_ELECTRON, SAMS_F_ENERGY_I
 
 struct sams_lare_server {
     sams::Batch batch;
+    int device = 0;
     long long budget = 0;
     long long in_use = 0;
     long long max_cells = 0;       // cap on running interior cells (0 = none)
@@ -78,8 +88,50 @@ struct sams_lare_server {
 
     void loop();
     bool admit_locked();
+    int admit_one(Request *r);
+    void drop(Request *r);
     void retire(Request *r, bool ok);
 };
+
+// Allocate r's solve (its own solver or a batch slot) and upload its
+// initial state.
+int sams_lare_server::admit_one(Request *r)
+{
+    int rc;
+    if (r->fused) {
+        r->solo.reset(new (std::nothrow) sams::Solver());
+        if (!r->solo) return SAMS_ERR_NOMEM;
+        rc = r->solo->init(r->p, r->bcs, device);
+        for (int f = 0; rc == SAMS_OK && f < SAMS_NFIELDS; ++f)
+            if (r->ic[f]) rc = r->solo->upload(f, r->ic[f], cudaMemcpyDefault);
+        if (rc == SAMS_OK) rc = r->solo->sync();
+        if (rc != SAMS_OK) {
+            worker_error = r->solo->err;
+            r->solo.reset();
+        }
+        return rc;
+    }
+    int slot = -1;
+    rc = batch.add(r->p, r->bcs, &slot);
+    for (int f = 0; rc == SAMS_OK && f < SAMS_NFIELDS; ++f)
+        if (r->ic[f]) rc = batch.upload(slot, f, r->ic[f], cudaMemcpyDefault);
+    if (rc == SAMS_OK) rc = batch.sync();
+    if (rc != SAMS_OK) {
+        if (slot >= 0) batch.remove(slot);
+        worker_error = batch.err;
+        return rc;
+    }
+    r->slot = slot;
+    return SAMS_OK;
+}
+
+// Free r's device memory (its solver or its batch slot).
+void sams_lare_server::drop(Request *r)
+{
+    if (r->solo) r->solo.reset();
+    else if (r->slot >= 0) batch.remove(r->slot);
+    r->slot = -1;
+}
 
 bool sams_lare_server::admit_locked()
 {
@@ -99,20 +151,12 @@ bool sams_lare_server::admit_locked()
             continue;
         }
         queue.pop_front();
-        int slot = -1;
-        int rc = batch.add(r->p, r->bcs, &slot);
-        for (int f = 0; rc == SAMS_OK && f < SAMS_NFIELDS; ++f)
-            if (r->ic[f]) rc = batch.upload(slot, f, r->ic[f], cudaMemcpyDefault);
-        if (rc == SAMS_OK) rc = batch.sync();
-        if (rc != SAMS_OK) {
-            if (slot >= 0) batch.remove(slot);
+        if (admit_one(r) != SAMS_OK) {
             r->status = SAMS_SERVE_FAILED;
             r->t_done = Clock::now();
             ++failed;
-            worker_error = batch.err;
             continue;
         }
-        r->slot = slot;
         r->status = SAMS_SERVE_RUNNING;
         r->t_admit = Clock::now();
         in_use += r->bytes;
@@ -133,10 +177,12 @@ void sams_lare_server::retire(Request *r, bool ok)
                 r->staged.emplace_back((size_t)n);
                 dst = r->staged.back().data();
             }
-            if (batch.download(r->slot, kStateFields[q], dst, cudaMemcpyDefault) != SAMS_OK) ok = false;
+            const int rc = r->solo ? r->solo->download(kStateFields[q], dst, cudaMemcpyDefault)
+                                   : batch.download(r->slot, kStateFields[q], dst, cudaMemcpyDefault);
+            if (rc != SAMS_OK) ok = false;
         }
     }
-    batch.remove(r->slot);
+    drop(r);
     r->t_done = Clock::now();
     std::lock_guard<std::mutex> lk(mu);
     in_use -= r->bytes;
@@ -165,7 +211,7 @@ void sams_lare_server::loop()
                     keep.push_back(r);
                     continue;
                 }
-                batch.remove(r->slot);
+                drop(r);
                 in_use -= r->bytes;
                 cells_in_use -= r->cells;
                 r->status = SAMS_SERVE_CANCELLED;
@@ -178,24 +224,34 @@ void sams_lare_server::loop()
             admit_locked();
         }
         if (running.empty()) continue;
-        // one batched step for every running solve
-        if (batch.step_graph(1) != SAMS_OK || batch.sync() != SAMS_OK) {
-            std::lock_guard<std::mutex> lk(mu);
-            worker_error = batch.err;
-            for (Request *r : running) {
-                batch.remove(r->slot);
+        // one step for every running solve: each fused-path solve launches
+        // its own step graph on its own stream, the others one batched step
+        std::vector<Request *> lost;  // solves whose step could not run
+        bool any_batched = false;
+        for (Request *r : running) {
+            if (!r->solo) any_batched = true;
+            else if (r->solo->step_graph(1) != SAMS_OK) lost.push_back(r);
+        }
+        bool batch_ok = !any_batched || (batch.step_graph(1) == SAMS_OK && batch.sync() == SAMS_OK);
+        if (!batch_ok) worker_error = batch.err;
+        for (Request *r : running)
+            if (r->solo && std::find(lost.begin(), lost.end(), r) == lost.end() &&
+                cudaStreamSynchronize(r->solo->stream()) != cudaSuccess)
+                lost.push_back(r);
+        std::vector<Request *> keep;
+        for (Request *r : running) {
+            if ((!r->solo && !batch_ok) || std::find(lost.begin(), lost.end(), r) != lost.end()) {
+                if (r->solo) worker_error = r->solo->err;
+                drop(r);
+                std::lock_guard<std::mutex> lk(mu);
                 in_use -= r->bytes;
                 cells_in_use -= r->cells;
                 r->status = SAMS_SERVE_FAILED;
                 r->t_done = Clock::now();
                 ++failed;
+                cv.notify_all();
+                continue;
             }
-            running.clear();
-            cv.notify_all();
-            continue;
-        }
-        std::vector<Request *> keep;
-        for (Request *r : running) {
             {
                 std::lock_guard<std::mutex> lk(mu);
                 r->done += 1;
@@ -204,8 +260,9 @@ void sams_lare_server::loop()
             bool finished = r->done >= r->nsteps;
             bool bad = false;
             if (finished || (r->done & 63) == 0) {
-                sams::Scalars s;
-                if (batch.scalars(r->slot, s) != SAMS_OK || s.status) bad = true;
+                sams::Scalars sc;
+                const int rc = r->solo ? r->solo->scalars(sc) : batch.scalars(r->slot, sc);
+                if (rc != SAMS_OK || sc.status) bad = true;
             }
             if (bad) retire(r, false);
             else if (finished) retire(r, true);
@@ -244,6 +301,7 @@ int sams_lare_serve_create(int device, int64_t budget_bytes, sams_lare_server **
         return rc;
     }
     s->budget = budget_bytes;
+    s->device = device;
     s->t_start = Clock::now();
     s->worker = std::thread([s, device] {
         cudaSetDevice(device);
@@ -271,7 +329,8 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
     for (int f = 0; f < SAMS_NFIELDS; ++f) r->ic[f] = ic[f];
     for (int q = 0; q < 9; ++q) r->out[q] = out ? out[q] : nullptr;
     r->nsteps = nsteps;
-    r->bytes = sams::Batch::bytes_for(*p);
+    r->fused = sams::Solver::fused_path(*p);
+    r->bytes = r->fused ? sams::Solver::bytes_for(*p) : sams::Batch::bytes_for(*p);
     r->cells = (long long)(p->nx * p->ny * p->nz);
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
@@ -290,7 +349,7 @@ int sams_lare_serve_submit(sams_lare_server *s, const sams_lare_params *p, const
 int sams_lare_serve_solve_bytes(const sams_lare_params *p, int64_t *bytes)
 {
     if (!p || !bytes) return SAMS_ERR_INVALID;
-    *bytes = (int64_t)sams::Batch::bytes_for(*p);
+    *bytes = (int64_t)(sams::Solver::fused_path(*p) ? sams::Solver::bytes_for(*p) : sams::Batch::bytes_for(*p));
     return SAMS_OK;
 }
 

@@ -686,6 +686,19 @@ bool lanes_full(long long n, long long w) { return 4 * n >= 3 * w * ceil_div(n, 
 
 // ---------------------------------------------------------------------------
 
+long long Solver::bytes_for(const sams_lare_params &p)
+{
+    const long long zrow = ((p.nz + 6) + 7) / 8 * 8;
+    const long long nelem = (p.nx + 5) * (p.ny + 5) * zrow;
+    const long long narr = SAMS_NFIELDS + NSCRATCH + (p.rke ? 1 : 0);
+    const long long staging = (p.nx + 5) * (p.ny + 5) * (p.nz + 5);
+    long long axes = 6 * (p.nx + p.ny + p.nz + 18);
+    if (p.geometry) axes += 5 * (p.nx + 6) * (p.ny + 6) + 8 * (p.nx + p.ny + 12);
+    return (narr * nelem + staging + axes) * (long long)sizeof(double) + (long long)sizeof(Scalars) + 4096;
+}
+
+bool Solver::fused_path(const sams_lare_params &p) { return lanes_full(p.nz + 1, kMK); }
+
 Solver::~Solver() { free_all(); }
 
 void Solver::free_all()

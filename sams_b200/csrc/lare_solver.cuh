@@ -55,6 +55,13 @@ public:
 
     // Returns a sams_status; on failure err holds the reason.
     int init(const sams_lare_params &p, const sams_lare_bcs &bcs, int device);
+    // Device bytes a solve of these parameters takes: state and scratch
+    // arrays, the host-transfer staging buffer, axes and metric tables (an
+    // upper bound, for admission under a memory budget).
+    static long long bytes_for(const sams_lare_params &p);
+    // Whether the step of a solve of these parameters runs the fused
+    // marching and windowed kernels (its z lines fill their tiles).
+    static bool fused_path(const sams_lare_params &p);
     // One x slab of a larger grid: p.nx is the slab's own cell count, the
     // x axis and metric tables are those of the whole grid (slab.nx_global
     // cells over x_min..x_max) from the slab's offset on.

@@ -134,3 +134,39 @@ def test_served_mix_with_a_192_cube_equals_solo():
             sl = lare.field_slices(f, *n)
             assert np.array_equal(out[q][sl], ref[f][sl]), f"{case}{n} {f}"
     srv.close()
+
+
+def test_own_stream_solves_fail_and_cancel_alone():
+    """Solves whose z lines fill the fused kernels (here nz = 24) step on
+    their own streams beside the batched ones.  One of them goes non-finite
+    and another is cancelled while running: both leave alone, and a fused
+    and a batched solve that share the GPU with them still equal their solo
+    runs bit for bit."""
+    srv = lare.Server(4 << 30)
+    p24, b24 = lare.case_setup("rf", 16, 12, 24)
+    p12, b12 = lare.case_setup("rf", 12, 12, 12)
+    bad = lare.case_fields("rf", p24, seed=1)
+    bad[0][:] = 0.0                       # zero density: the CFL timestep is not finite
+    tb = srv.submit(p24, b24, bad, 70)
+    long_run = srv.submit(p24, b24, lare.case_fields("rf", p24, seed=2), 100000)
+    out24 = [np.zeros(lare.box_shape(16, 12, 24)) for _ in range(9)]
+    out12 = [np.zeros(lare.box_shape(12, 12, 12)) for _ in range(9)]
+    g24 = srv.submit(p24, b24, lare.case_fields("rf", p24, seed=3), 9, out24)
+    g12 = srv.submit(p12, b12, lare.case_fields("rf", p12, seed=4), 11, out12)
+    for _ in range(2000):
+        if srv.poll(long_run)[0] == "running":
+            break
+        time.sleep(0.005)
+    srv.cancel(long_run)
+    srv.drain(300)
+    assert srv.poll(tb)[0] == "failed"
+    assert srv.poll(long_run)[0] == "cancelled"
+    for t, out, n, steps, seed in ((g24, out24, (16, 12, 24), 9, 3), (g12, out12, (12, 12, 12), 11, 4)):
+        assert srv.poll(t)[0] == "done"
+        ref = _solo("rf", n, steps, seed)
+        for q, f in enumerate(STATE):
+            sl = lare.field_slices(f, *n)
+            assert np.array_equal(out[q][sl], ref[f][sl]), f"{n} {f}"
+    st = srv.stats()
+    assert st["completed"] == 2 and st["failed"] == 1
+    srv.close()
