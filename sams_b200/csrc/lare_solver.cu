@@ -65,7 +65,7 @@ constexpr int kZThreads = ops::kZLineThreads;
 // (SweepCTUpd<2> with that argument), which nothing else in the kernel reads
 // or writes.
 template <bool GEO>
-__global__ void __launch_bounds__(kZThreads, 4) k_zsweep(Ctx c, int ct_arg)  // 4 blocks per SM, tuned on B200
+__global__ void __launch_bounds__(kZThreads, 5) k_zsweep(Ctx c, int ct_arg)  // 5 blocks per SM, tuned on B200
 {
     using F = ops::SweepFused<2>;
     extern __shared__ double zsm[];
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kMThreads, P::kMinBlocks) k_cellnode_march(Ctx
 // the node averages, so cs never goes to global memory; in resistive runs
 // (arg 1) the cell's step-start p_e, p_i are stored.
 struct PrepMarch {
-    static constexpr int NR = 2, kMinBlocks = 4;  // register cap tuned on B200
+    static constexpr int NR = 2, kMinBlocks = 5;  // register cap tuned on B200
     template <bool GEO, bool P2>
     __device__ static void produce(const Ctx &c, int resistive, int i, int j, int k, bool own, double *out)
     {
@@ -273,7 +273,7 @@ struct PrepMarch {
 // volumes cvc1.
 template <int DIR>
 struct VolMarch {
-    static constexpr int NR = 1, kMinBlocks = 4;
+    static constexpr int NR = 1, kMinBlocks = DIR == 2 ? 5 : 4;  // register cap tuned on B200
     template <bool GEO, bool P2>
     __device__ static void produce(const Ctx &c, int arg, int i, int j, int k, bool own, double *out)
     {
@@ -425,7 +425,7 @@ struct CtStore {
 };
 
 template <int DIR, bool GEO>
-__global__ void __launch_bounds__(ops::kWinThreads, 6) k_ctmass(Ctx c, int scale)
+__global__ void __launch_bounds__(ops::kWinThreads, 5) k_ctmass(Ctx c, int scale)  // cap tuned on B200
 {
     using F = ops::SweepCTMass<DIR>;
     constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
@@ -462,7 +462,7 @@ struct ZRowStore {
 };
 
 template <bool GEO>
-__global__ void __launch_bounds__(256, 6) k_ctmass_z(Ctx c)
+__global__ void __launch_bounds__(256, 5) k_ctmass_z(Ctx c)  // cap tuned on B200
 {
     using F = ops::SweepCTMass<2>;
     __shared__ double zsm[F::NARR * kZRows * kZSpan];
