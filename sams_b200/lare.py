@@ -442,8 +442,10 @@ def route_pick(pending_cell_updates, committed_bytes, budget_bytes, request_byte
 class Server:
     """Continuous-batching LARE3D server on one GPU (include/sams_lare.h,
     serving section).  Submitted solves are admitted as device memory within
-    `budget_bytes` frees up, stepped together with every other running solve,
-    and their final state copied back when their step count is reached."""
+    `budget_bytes` frees up, stepped together with every other running solve
+    (large ones on their own streams, small and thin ones in one batched
+    step), and their final state copied back when their step count is
+    reached."""
 
     _prefix = "sams_lare_serve_"
 
