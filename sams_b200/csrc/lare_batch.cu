@@ -123,11 +123,13 @@ __global__ void __launch_bounds__(ops::kZLineThreads, 4)
         const bool on = line < lines && q < (long long)(g.nx + 1) * (g.ny + 1);
         const int i = on ? (int)(q / (g.ny + 1)) : 0, j = on ? (int)(q % (g.ny + 1)) : 0;
         using F = ops::SweepFused<2>;
+        static_assert(!F::kSharedFluxSlots, "the z passes of stage B run without a barrier between them");
         const ops::LineStore st{zsm, S, line * W + k + 2};
         const ops::SweepOut w = ops::sweep_in_place(c);
         if (on) F::stage_a<GEO>(c, i, j, k, st, w, true);
         __syncthreads();
-        if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st, w, true);
+        if (on && k >= 1 && k <= g.nz) F::stage_b_energy(c, i, j, k, st, w);
+        if (on && k >= -1 && k <= g.nz) F::stage_b_mom<GEO>(c, i, j, k, st);  // its own slots: no barrier between
         __syncthreads();
         if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st, w);
     }

@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kZThreads, 5) k_zsweep(Ctx c, int ct_arg)  // 
 {
     using F = ops::SweepFused<2>;
     extern __shared__ double zsm[];
+    static_assert(!F::kSharedFluxSlots, "the z passes of stage B run without a barrier between them");
     const Geom &g = c.g;
     const int W = g.nz + 4, lines = kZThreads / W, S = lines * W;
     const int line = (int)threadIdx.x / W, k = (int)threadIdx.x % W - 2;
@@ -79,7 +80,8 @@ __global__ void __launch_bounds__(kZThreads, 5) k_zsweep(Ctx c, int ct_arg)  // 
     const ops::SweepOut w = ops::sweep_in_place(c);
     if (on) F::stage_a<GEO>(c, i, j, k, st, w, true);
     __syncthreads();
-    if (on && k >= -1 && k <= g.nz) F::stage_b<GEO>(c, i, j, k, st, w, true);
+    if (on && k >= 1 && k <= g.nz) F::stage_b_energy(c, i, j, k, st, w);
+    if (on && k >= -1 && k <= g.nz) F::stage_b_mom<GEO>(c, i, j, k, st);  // its own slots: no barrier between
     __syncthreads();
     if (on && k >= 0 && k <= g.nz) F::stage_c(c, i, j, k, st, w);
     if (ct_arg >= 0 && on && k >= 0 && k <= g.nz) ops::SweepCTUpd<2>::run<GEO, false>(c, ct_arg, i, j, k);
@@ -113,9 +115,12 @@ __global__ void __launch_bounds__(ops::kWinThreads, 4) k_psweep(Ctx c, ops::Swee
     for (int s = a_lo + sl; s <= a_hi; s += TS)
         if (on) F::template stage_a<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w, s >= s0 && s <= s1);
     __syncthreads();
+    for (int s = s0 + sl; s <= s1; s += TS)
+        if (on) F::stage_b_energy(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w);
+    __syncthreads();
     const int b_lo = max(s0 - 1, -1);
     for (int s = b_lo + sl; s <= s1; s += TS)
-        if (on) F::template stage_b<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w, s >= s0);
+        if (on) F::template stage_b_mom<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s));
     __syncthreads();
     for (int s = s0 + sl; s <= s1; s += TS)
         if (on) F::stage_c(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), w);
