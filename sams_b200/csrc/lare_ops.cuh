@@ -106,6 +106,7 @@ __host__ __device__ inline void set_bounds(int *lo, int *hi, int a0, int b0, int
 // src(arr, q) is array arr at offset q.  (The fused kernels read the same
 // values from a shared-memory ring instead.)
 struct ArraySrc {
+    static constexpr bool kPressureSum = false;  // p_e and p_i are separate arrays (see Pred2)
     const double *a[6];
     __device__ double operator()(int arr, int q) const { return __ldg(a[arr] + q); }
 };
@@ -635,6 +636,9 @@ struct Pred2 {
             __device__ double operator[](int q) const { return s(a, q); }
         };
         const Arr pe{src, Pred1::PE}, pi{src, Pred1::PI}, cv1{src, Pred1::CV1};
+        // p_e + p_i of cell q: a source with kPressureSum holds that sum (the
+        // same addition, made where the values were produced) under PE
+        auto ptot = [&](int q) { return S::kPressureSum ? pe[q] : pe[q] + pi[q]; };
         const Arr bx1{src, Pred1::B1X}, by1{src, Pred1::B1Y}, bz1{src, Pred1::B1Z};
         const double dx = c.ax.dxc[i + 2], dy = c.ax.dyc[j + 2], dz = c.ax.dzc[k + 2];
         // metric factors (lagran.cpp:627-630; all 1.0 in Cartesian geometry)
@@ -652,8 +656,8 @@ struct Pred2 {
         const double dhy = geo ? h2c * dy : dy, dhz = geo ? h3c * dz : dz;
         const int qx = q0 + QX, qy = q0 + QY, qz = q0 + QZ, qxy = q0 + QX + QY, qxz = q0 + QX + QZ,
                   qyz = q0 + QY + QZ, qxyz = q0 + QX + QY + QZ;
-        double pp = pe[q0] + pi[q0], ppx = pe[qx] + pi[qx], ppy = pe[qy] + pi[qy], ppz = pe[qz] + pi[qz];
-        double ppxy = pe[qxy] + pi[qxy], ppxz = pe[qxz] + pi[qxz], ppyz = pe[qyz] + pi[qyz], ppxyz = pe[qxyz] + pi[qxyz];
+        double pp = ptot(q0), ppx = ptot(qx), ppy = ptot(qy), ppz = ptot(qz);
+        double ppxy = ptot(qxy), ppxz = ptot(qxz), ppyz = ptot(qyz), ppxyz = ptot(qxyz);
         double w1 = pp + ppy + ppz + ppyz;
         double w2 = ppx + ppxy + ppxz + ppxyz;
         double fx = div_by<P2>((w1 - w2) * 0.25, dx, c.rc.xc);
@@ -1224,7 +1228,7 @@ struct SweepMass {
 // fluxes() at the window's own points.
 template <int DIR>
 struct SweepCTMass {
-    enum { F1, F2, DB1, DB2, NARR };  // the two quotients and their db averages
+    enum { F1, F2, DB1, DB2, NARR };
     // t1 / t2: transverse offset of the db1 sample averaged for flux 1 / 2;
     // va1 / va2: offset of the second v1 sample of its advection velocity
     __device__ static void offsets(const Geom &g, int &t1, int &t2, int &va1, int &va2)
@@ -1252,8 +1256,6 @@ struct SweepCTMass {
         }
         st.put(F1, v1 / dba1);
         st.put(F2, v2 / dba2);
-        st.put(DB1, dba1);
-        st.put(DB2, dba2);
     }
     // CT fluxes where `ct` ((i, j, k) in 0..n), the mass flux everywhere it
     // is called (0..n along the sweep, 0..n+1 across)
@@ -1269,12 +1271,14 @@ struct SweepCTMass {
         if (ct) {
             int t1, t2, va1, va2;
             offsets(g, t1, t2, va1, va2);
-            const RO v1{c.f[SAMS_F_VX1 + DIR]};
+            const RO v1{c.f[SAMS_F_VX1 + DIR]}, db1{c.s[S_R_DB1]};
             const double v1o = v1[o];
+            const double dbi1 = (db1[o] + db1[o + t1]) * 0.5, dbp1 = (db1[o + d] + db1[o + d + t1]) * 0.5;
+            const double dbi2 = (db1[o] + db1[o + t2]) * 0.5, dbp2 = (db1[o + d] + db1[o + d + t2]) * 0.5;
             c.s[S_R_CT1][o] = ct_flux_q((v1o + v1[o + va1]) * 0.5, dt, st.get(F1, -1), st.get(F1, 0), st.get(F1, 1),
-                                        st.get(F1, 2), st.get(DB1, 0), st.get(DB1, 1), dci, dcm, dcp, cvi, cvp);
+                                        st.get(F1, 2), dbi1, dbp1, dci, dcm, dcp, cvi, cvp);
             c.s[S_R_CT2][o] = ct_flux_q((v1o + v1[o + va2]) * 0.5, dt, st.get(F2, -1), st.get(F2, 0), st.get(F2, 1),
-                                        st.get(F2, 2), st.get(DB2, 0), st.get(DB2, 1), dci, dcm, dcp, cvi, cvp);
+                                        st.get(F2, 2), dbi2, dbp2, dci, dcm, dcp, cvi, cvp);
         }
         const RO rho{c.f[SAMS_F_RHO]};
         c.f[SAMS_F_DM][o] = mass_flux(face_velocity<DIR>(c, o), dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d],

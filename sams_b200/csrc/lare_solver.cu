@@ -148,6 +148,15 @@ constexpr int kRP = (kMK + 1) * (kMJ + 1);  // cells of one ring plane
 constexpr int kMThreads = (kRP + 31) / 32 * 32;
 
 struct RingSrc {
+    static constexpr bool kPressureSum = false;
+    const double *ring;
+    __device__ double operator()(int arr, int q) const { return ring[arr * 3 * kRP + q]; }
+};
+// The predictor's ring: Pred1's outputs with p_e + p_i in the PE slot (Pred2
+// reads only that sum), five arrays.
+struct PredRingSrc {
+    static constexpr bool kPressureSum = true;
+    static constexpr int NR = ops::Pred1::PI;  // CV1, B1X, B1Y, B1Z, PE (= p_e + p_i)
     const double *ring;
     __device__ double operator()(int arr, int q) const { return ring[arr * 3 * kRP + q]; }
 };
@@ -156,7 +165,7 @@ template <bool GEO, bool P2>
 __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistive, double *pe_out, double *pi_out)
 {
     using P1 = ops::Pred1;
-    extern __shared__ double ring[];  // [P1::NOUT][3 planes][kRP]
+    extern __shared__ double ring[];  // [PredRingSrc::NR][3 planes][kRP]
     const Geom &g = c.g;
     const int nkt = (g.nz + kMK) / kMK, njt = (g.ny + kMJ) / kMJ;  // tiles over nodes 0..n
     int b = (int)blockIdx.x;
@@ -177,7 +186,8 @@ __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistiv
             bool half_p;
             P1::compute<GEO, P2>(c, resistive, i, j, k, out, half_p);
 #pragma unroll
-            for (int a = 0; a < P1::NOUT; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
+            for (int a = 0; a < P1::PE; ++a) ring[(a * 3 + slot) * kRP + p] = out[a];
+            ring[(P1::PE * 3 + slot) * kRP + p] = out[P1::PE] + out[P1::PI];
             if (pj < kMJ && pk < kMK && i <= i1 && j <= g.ny && k <= g.nz) {
                 const int o = box_off(g, i, j, k);
                 pe_out[o] = out[P1::PE];
@@ -188,7 +198,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_pred_march(Ctx c, int resistiv
     const int kc = t % (kMK + 1), jc = t / (kMK + 1);
     const int j = j0 + jc, k = k0 + kc;
     const bool on = kc < kMK && jc < kMJ && j <= g.ny && k <= g.nz;
-    const RingSrc src{ring};
+    const PredRingSrc src{ring};
     produce(i0);
     for (int i = i0; i <= i1; ++i) {
         produce(i + 1);
@@ -1080,7 +1090,7 @@ void Solver::launch_pred(int resistive)
 {
     const Geom &g = ctx_.g;
     const long long blocks = (long long)((g.nz + kMK) / kMK) * ((g.ny + kMJ) / kMJ) * ((g.nx + kMI) / kMI);
-    const size_t smem = (size_t)ops::Pred1::NOUT * 3 * kRP * sizeof(double);
+    const size_t smem = (size_t)PredRingSrc::NR * 3 * kRP * sizeof(double);
     double *pe = ctx_.s[S_CS], *pi = ctx_.s[S_CSV];
     if (ctx_.p.geometry)
         k_pred_march<true, false><<<(unsigned)blocks, kMThreads, smem, stream_>>>(ctx_, resistive, pe, pi);
