@@ -1228,7 +1228,7 @@ struct SweepMass {
 // fluxes() at the window's own points.
 template <int DIR>
 struct SweepCTMass {
-    enum { F1, F2, DB1, DB2, NARR };
+    enum { F1, F2, DB1, DB2, NARR };  // the two quotients and their db averages
     // t1 / t2: transverse offset of the db1 sample averaged for flux 1 / 2;
     // va1 / va2: offset of the second v1 sample of its advection velocity
     __device__ static void offsets(const Geom &g, int &t1, int &t2, int &va1, int &va2)
@@ -1256,6 +1256,8 @@ struct SweepCTMass {
         }
         st.put(F1, v1 / dba1);
         st.put(F2, v2 / dba2);
+        st.put(DB1, dba1);
+        st.put(DB2, dba2);
     }
     // CT fluxes where `ct` ((i, j, k) in 0..n), the mass flux everywhere it
     // is called (0..n along the sweep, 0..n+1 across)
@@ -1271,14 +1273,12 @@ struct SweepCTMass {
         if (ct) {
             int t1, t2, va1, va2;
             offsets(g, t1, t2, va1, va2);
-            const RO v1{c.f[SAMS_F_VX1 + DIR]}, db1{c.s[S_R_DB1]};
+            const RO v1{c.f[SAMS_F_VX1 + DIR]};
             const double v1o = v1[o];
-            const double dbi1 = (db1[o] + db1[o + t1]) * 0.5, dbp1 = (db1[o + d] + db1[o + d + t1]) * 0.5;
-            const double dbi2 = (db1[o] + db1[o + t2]) * 0.5, dbp2 = (db1[o + d] + db1[o + d + t2]) * 0.5;
             c.s[S_R_CT1][o] = ct_flux_q((v1o + v1[o + va1]) * 0.5, dt, st.get(F1, -1), st.get(F1, 0), st.get(F1, 1),
-                                        st.get(F1, 2), dbi1, dbp1, dci, dcm, dcp, cvi, cvp);
+                                        st.get(F1, 2), st.get(DB1, 0), st.get(DB1, 1), dci, dcm, dcp, cvi, cvp);
             c.s[S_R_CT2][o] = ct_flux_q((v1o + v1[o + va2]) * 0.5, dt, st.get(F2, -1), st.get(F2, 0), st.get(F2, 1),
-                                        st.get(F2, 2), dbi2, dbp2, dci, dcm, dcp, cvi, cvp);
+                                        st.get(F2, 2), st.get(DB2, 0), st.get(DB2, 1), dci, dcm, dcp, cvi, cvp);
         }
         const RO rho{c.f[SAMS_F_RHO]};
         c.f[SAMS_F_DM][o] = mass_flux(face_velocity<DIR>(c, o), dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d],
