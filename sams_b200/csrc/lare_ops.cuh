@@ -417,8 +417,12 @@ struct ResistRK {
         double jz1 = div_by<P2>(by[o + SX] - by[o], dxc, rx) - div_by<P2>(bx[o + SY] - bx[o], dyc, ry);
         double jz2 = div_by<P2>(by[o + SX + 1] - by[o + 1], dxc, rx) - div_by<P2>(bx[o + SY + 1] - bx[o + 1], dyc, ry);
         double jx = 0.5 * (jx1 + jx2), jy = 0.5 * (jy1 + jy2), jz = 0.5 * (jz1 + jz2);
-        double j_local = sqrt(jx * jx + jy * jy + jz * jz);
-        double eta = j_local > c.p.j_max ? c.p.eta_bg + c.p.eta0 : c.p.eta_bg;
+        // eta_bg + eta0 where |J| > j_max, else eta_bg.  When the two have the
+        // same bits (eta0 = 0: the configurations' uniform eta) the choice
+        // cannot show and the square root of |J|^2 is skipped.
+        const double eta_hi = c.p.eta_bg + c.p.eta0;
+        const bool same = __double_as_longlong(eta_hi) == __double_as_longlong(c.p.eta_bg);
+        double eta = !same && sqrt(jx * jx + jy * jy + jz * jz) > c.p.j_max ? eta_hi : c.p.eta_bg;
         out[FX] = -jx * eta * dxc * 0.5;
         out[FY] = -jy * eta * dyc * 0.5;
         out[FZ] = -jz * eta * dzc * 0.5;

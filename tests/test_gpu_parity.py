@@ -216,3 +216,25 @@ def test_gpu_lare_other_bcs_match_checker(case, n, steps, oracle_lib):
         assert s.dt == o.dt
     _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"lare bcs {case}{n}")
     s.close()
+
+
+@pytest.mark.parametrize("n,j_max", [((16, 12, 24), 0.5), ((16, 12, 24), 1.0), ((12, 10, 6), 2.0)])
+def test_gpu_matches_checker_with_current_dependent_eta(n, j_max, oracle_lib):
+    """eta = eta_bg + eta0 where |J| > j_max (lagran.cpp:445-476), on a grid
+    with the fused resistive march (nz = 24) and a thin one, against the
+    checker bit for bit.  (The configurations use eta0 = 0, where the
+    kernels skip |J|'s square root.)"""
+    lo = oracle_lib
+    nx, ny, nz = n
+    p, b = lare.case_setup("rf", nx, ny, nz)
+    p.eta0, p.j_max = 2e-3, j_max
+    s = lare.LARE3D(p, b)
+    s.upload_all(lare.case_fields("rf", p, seed=9))
+    po, bo = lo.case_setup("rf", nx, ny, nz)
+    po.eta0, po.j_max = 2e-3, j_max
+    o = lo.Oracle(po, bo, lo.case_fields("rf", po, seed=9))
+    for _ in range(4):
+        s.step(1, graph=True)
+        o.step(1)
+        assert s.dt == o.dt
+    _assert_state_equal(s, lambda f: _masked(o.field(f), f, nx, ny, nz), f"rf{n} j_max {j_max}")
