@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kT, (MinBlocksBatch<Op, P2>::value))
 }
 
 template <bool GEO, bool P2>
-__global__ void __launch_bounds__(kT, (MinBlocksBatch<ops::Visc, P2>::value))
+__global__ void __launch_bounds__(kT, 4)  // the split work at 4 blocks per SM, as k_visc_split
     kb_visc(const Ctx *__restrict__ ctxs, const Tile *__restrict__ tiles, int ntiles, int tile_i)
 {
     __shared__ Ctx c;
@@ -77,15 +77,22 @@ __global__ void __launch_bounds__(kT, (MinBlocksBatch<ops::Visc, P2>::value))
         __syncthreads();
         load_ctx(c, ctxs + tl.inst);
         __syncthreads();
-        const int p = tl.p0 + (int)threadIdx.x;
+        // two threads per cell, as the single-solve k_visc_split: warps 0-3
+        // run the heating and forces, warps 4-7 the viscous pressure and CFL
+        // candidate, each over the tile's points in two rounds of 128
+        const int half = (int)threadIdx.x >> 7;
         double best = DBL_MAX;
         bool bad = false;
-        if (p < (hi[1] - lo[1] + 1) * nk) {
+        for (int r = 0; r < 2; ++r) {
+            const int p = tl.p0 + r * (kT / 2) + ((int)threadIdx.x & (kT / 2 - 1));
+            if (p >= (hi[1] - lo[1] + 1) * nk) continue;
             const int j = lo[1] + p / nk, k = lo[2] + p % nk;
             const int ia = max(tl.i0, lo[0]), ib = min(tl.i0 + tile_i - 1, hi[0]);
             for (int i = ia; i <= ib; ++i) {
-                double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
-                best = dev::pmin(best, cand);
+                if (half == 0)
+                    ops::Visc::template heat_forces<GEO, P2>(c, i, j, k, bad);
+                else if (i <= c.g.nx && j <= c.g.ny && k <= c.g.nz)
+                    best = dev::pmin(best, ops::Visc::template cfl<GEO, P2>(c, i, j, k, bad));
             }
         }
         if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c.sc->status, 1);

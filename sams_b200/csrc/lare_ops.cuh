@@ -260,16 +260,19 @@ struct Alpha {
 // cell's CFL candidate (p_visc is consumed here and never stored).
 // Returns the candidate (DBL_MAX outside the CFL range).
 struct Visc {
-    static constexpr int kMinBlocks = 3;  // blocks of 256 per SM (register cap), tuned on B200
+    // (launched by k_visc_split and kb_visc, each with its own register cap)
     __host__ __device__ static void bounds(const Geom &g, int, int *lo, int *hi)
     {
         set_bounds(lo, hi, 0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1);
     }
-    // nonfinite is set when a NaN or infinity shows up in this cell's viscous
-    // pressure, heating or CFL terms (the solve's state is no longer finite;
-    // the min itself would hide it, as LARE's min does).
+    // The cell's work in two halves, which the single-solve kernel
+    // (k_visc_split) gives to different threads: heat_forces is the viscous
+    // heating of cell (i, j, k) (lagran.cpp:283-326) and the viscous forces
+    // on node (i, j, k) (:329-376); cfl is the cell's viscous pressure
+    // (:303-305, with the three edge jumps it needs formed again, the same
+    // expressions) and its CFL candidate (set_dt, :380-443).
     template <bool GEO, bool P2>
-    __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
+    __device__ static void heat_forces(const Ctx &c, int i, int j, int k, bool &nonfinite)
     {
         const Geom &g = c.g;
         const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
@@ -297,10 +300,6 @@ struct Visc {
         double a11 = DV2(c_mmm, c_mm0);
         double a12 = DV2(c_0mm, c_0m0);
 #undef DV2
-        double p_visc = 0.0;
-        p_visc = pmax(p_visc, -a1a[o] * sqrt(a1));
-        p_visc = pmax(p_visc, -a2a[o] * sqrt(a2));
-        p_visc = pmax(p_visc, -a3a[o] * sqrt(a9));
         double vh = -0.25 * dy * dz * a1a[o] * a1
                     - 0.25 * dx * dz * a2a[o] * a2
                     - 0.25 * dy * dz * a1a[o + SY] * a3
@@ -315,29 +314,47 @@ struct Visc {
                     - 0.25 * dx * dy * a3a[o - SY] * a12;
         const double cv = (GEO && c.p.geometry) ? cv_at<GEO>(c, i, j, k) : dx * (dyp * dzp);
         c.s[S_VH][o] = div_by<P2>(vh, cv, c.rc.cv);
-        if (i > g.nx || j > g.ny || k > g.nz) return DBL_MAX;
-
-        // viscous forces on node (i, j, k)
-        {
-            double e1 = a1a[o + SY + 1] * dy * dz;
-            double e2 = a1a[o + SX + SY + 1] * dy * dz;
-            double e3 = a2a[o + 1] * dx * dz;
-            double e4 = a2a[o + SY + 1] * dx * dz;
-            double e5 = a3a[o] * dx * dy;
-            double e6 = a3a[o + 1] * dx * dy;
-            // cv_v = 0.125 * (8-cell sum of cv) (lagran.cpp:142-151)
-            const int ip = i + 1, jp = j + 1, kp = k + 1;
-            double sum_cv = cv_at<GEO>(c, i, j, k) + cv_at<GEO>(c, ip, j, k) + cv_at<GEO>(c, i, jp, k) + cv_at<GEO>(c, ip, jp, k) +
-                            cv_at<GEO>(c, i, j, kp) + cv_at<GEO>(c, ip, j, kp) + cv_at<GEO>(c, i, jp, kp) + cv_at<GEO>(c, ip, jp, kp);
-            double cv_v = 0.125 * sum_cv;
+        if (i > g.nx || j > g.ny || k > g.nz) return;
+        // checked where run checks it: the cells of the CFL range
+        if (!(GEO && c.p.geometry && i < 1) && !(fabs(vh) <= DBL_MAX)) nonfinite = true;
+        double e1 = a1a[o + SY + 1] * dy * dz;
+        double e2 = a1a[o + SX + SY + 1] * dy * dz;
+        double e3 = a2a[o + 1] * dx * dz;
+        double e4 = a2a[o + SY + 1] * dx * dz;
+        double e5 = a3a[o] * dx * dy;
+        double e6 = a3a[o + 1] * dx * dy;
+        // cv_v = 0.125 * (8-cell sum of cv) (lagran.cpp:142-151)
+        const int ip = i + 1, jp = j + 1, kp = k + 1;
+        double sum_cv = cv_at<GEO>(c, i, j, k) + cv_at<GEO>(c, ip, j, k) + cv_at<GEO>(c, i, jp, k) + cv_at<GEO>(c, ip, jp, k) +
+                        cv_at<GEO>(c, i, j, kp) + cv_at<GEO>(c, ip, j, kp) + cv_at<GEO>(c, i, jp, kp) + cv_at<GEO>(c, ip, jp, kp);
+        double cv_v = 0.125 * sum_cv;
 #define FV(v) div_by<P2>(e1 * (v[o] - v[o - SX]) + e2 * (v[o] - v[o + SX]) + e3 * (v[o] - v[o - SY]) + \
                 e4 * (v[o] - v[o + SY]) + e5 * (v[o] - v[o - 1]) + e6 * (v[o] - v[o + 1]), cv_v, c.rc.cv)
-            c.s[S_FXV][o] = FV(vx);
-            c.s[S_FYV][o] = FV(vy);
-            c.s[S_FZV][o] = FV(vz);
+        c.s[S_FXV][o] = FV(vx);
+        c.s[S_FYV][o] = FV(vy);
+        c.s[S_FZV][o] = FV(vz);
 #undef FV
-        }
-        // CFL candidate of cell (i, j, k) (lagran.cpp:388-438)
+    }
+    // (cells 0..n; DBL_MAX outside the CFL range)
+    template <bool GEO, bool P2>
+    __device__ static double cfl(const Ctx &c, int i, int j, int k, bool &nonfinite)
+    {
+        const Geom &g = c.g;
+        const RO vx{c.f[SAMS_F_VX]}, vy{c.f[SAMS_F_VY]}, vz{c.f[SAMS_F_VZ]};
+        const RO a1a{c.s[S_A1]}, a2a{c.s[S_A2]}, a3a{c.s[S_A3]};
+        const int SX = g.sx, SY = g.sy;
+        const int o = LOFF(i, j, k);
+        const double dx = c.ax.dxb[i + 2], dyp = c.ax.dyb[j + 2], dzp = c.ax.dzb[k + 2];
+#define DV2(a, b) ((vx[a] - vx[b]) * (vx[a] - vx[b]) + (vy[a] - vy[b]) * (vy[a] - vy[b]) + (vz[a] - vz[b]) * (vz[a] - vz[b]))
+        const int c_mmm = o - SX - SY - 1, c_0mm = o - SY - 1, c_00m = o - 1, c_m0m = o - SX - 1;
+        const int c_mm0 = o - SX - SY, c_0m0 = o - SY, c_000 = o, c_m00 = o - SX;
+        const double a1 = DV2(c_mmm, c_0mm), a2 = DV2(c_0mm, c_00m), a9 = DV2(c_00m, c_000);
+#undef DV2
+        double p_visc = 0.0;
+        p_visc = pmax(p_visc, -a1a[o] * sqrt(a1));
+        p_visc = pmax(p_visc, -a2a[o] * sqrt(a2));
+        p_visc = pmax(p_visc, -a3a[o] * sqrt(a9));
+        const double cv = (GEO && c.p.geometry) ? cv_at<GEO>(c, i, j, k) : dx * (dyp * dzp);
         const double gm = c.p.gamma;
         const RO bx{c.f[SAMS_F_BX]}, by{c.f[SAMS_F_BY]}, bz{c.f[SAMS_F_BZ]};
         double rho = __ldg(c.f[SAMS_F_RHO] + o);
@@ -373,9 +390,19 @@ struct Visc {
         double dt2 = volume / pmax(pmax(pmax(avxm, avxp), dvx), 1.0e-10 * volume);
         double dt3 = volume / pmax(pmax(pmax(avym, avyp), dvy), 1.0e-10 * volume);
         double dt4 = volume / pmax(pmax(pmax(avzm, avzp), dvz), 1.0e-10 * volume);
-        const double chk = dt1 + dt2 + dt3 + dt4 + p_visc + vh;
+        const double chk = dt1 + dt2 + dt3 + dt4 + p_visc;
         if (!(fabs(chk) <= DBL_MAX)) nonfinite = true;
         return pmin(pmin(pmin(dt1, dt2), dt3), dt4);
+    }
+    // nonfinite is set when a NaN or infinity shows up in this cell's viscous
+    // pressure, heating or CFL terms (the solve's state is no longer finite;
+    // the min itself would hide it, as LARE's min does).
+    template <bool GEO, bool P2>
+    __device__ static double run(const Ctx &c, int, int i, int j, int k, bool &nonfinite)
+    {
+        heat_forces<GEO, P2>(c, i, j, k, nonfinite);
+        if (i > c.g.nx || j > c.g.ny || k > c.g.nz) return DBL_MAX;
+        return cfl<GEO, P2>(c, i, j, k, nonfinite);
     }
 };
 
@@ -1742,10 +1769,6 @@ struct CapP2 {
     static constexpr int value = Op::kMinBlocks;
 };
 template <>
-struct CapP2<Visc> {
-    static constexpr int value = 2;
-};
-template <>
 struct CapP2<NodePrep> {
     static constexpr int value = 5;
 };
@@ -1766,7 +1789,6 @@ template <class Op>
 struct CapBatch {
     static constexpr int value = Op::kMinBlocks;
 };
-template <> struct CapBatch<Visc> { static constexpr int value = 4; };
 template <> struct CapBatch<BScale> { static constexpr int value = 8; };
 template <> struct CapBatch<SweepCvc> { static constexpr int value = 8; };
 template <> struct CapBatch<Corr2> { static constexpr int value = 5; };

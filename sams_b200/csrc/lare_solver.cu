@@ -4,8 +4,8 @@
 // the standard path: Cartesian or curvilinear, no rke, every dimension at
 // least three cells, every B edge with a condition):
 //   [startOfTimestep -> lagrangian_step, lagran.cpp:95-173]
-//     k_cellnode_march (CellPrep + NodePrep), Alpha, Visc (+ CFL block
-//     minima), DtFinalize, resistive only: 2 x {k_resist_march (ResistRK +
+//     k_cellnode_march (CellPrep + NodePrep), Alpha, k_visc_split (Visc +
+//     CFL block minima), DtFinalize, resistive only: 2 x {k_resist_march (ResistRK +
 //     ResistB), fill B + energies}, k_pred_march (Pred1 + Pred2), fill v1
 //   [halfTimestep -> corrector_step, lagran.cpp:739-804]
 //     k_edge_march (Corr1 from per-node edge terms), Corr2, fill v +
@@ -528,16 +528,22 @@ __global__ void __launch_bounds__(kThreads) k_copy_shell(Ctx c, ops::SweepOut w)
     }
 }
 
-// Visc with the CFL minimum: each block reduces its candidates and folds
-// them into Scalars::dtmin_bits.  Positive doubles order like their bit
-// patterns, so an integer atomicMin is an exact, order-free minimum.
+// Visc with two threads per cell: a block holds 128 cells of a plane row,
+// its first four warps run the viscous heating and forces
+// (ops::Visc::heat_forces), the other four the viscous pressure and CFL
+// candidate (ops::Visc::cfl), so each thread carries half the work's live
+// values.  Both halves read the same corners, which the block's L1 serves.
+// The block's minimum candidate goes to Scalars::dtmin_bits: positive
+// doubles order like their bit patterns, so an integer atomicMin is an
+// exact, order-free minimum.
 template <bool GEO, bool P2>
-__global__ void __launch_bounds__(kThreads, (MinBlocks<ops::Visc, P2>::value)) k_visc(Ctx c)
+__global__ void __launch_bounds__(kThreads, 4) k_visc_split(Ctx c)  // 4 blocks per SM, tuned on B200
 {
     int lo[3], hi[3];
     ops::Visc::bounds(c.g, 0, lo, hi);
     const int nk = hi[2] - lo[2] + 1;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int half = (int)threadIdx.x >> 7;
+    const long long t = (long long)blockIdx.x * (kThreads / 2) + (threadIdx.x & (kThreads / 2 - 1));
     const long long plane = (long long)(hi[1] - lo[1] + 1) * nk;
     double best = DBL_MAX;
     bool bad = false;
@@ -545,8 +551,10 @@ __global__ void __launch_bounds__(kThreads, (MinBlocks<ops::Visc, P2>::value)) k
         const int j = lo[1] + (int)(t / nk);
         const int k = lo[2] + (int)(t % nk);
         for (int i = lo[0] + (int)blockIdx.y; i <= hi[0]; i += gridDim.y) {
-            double cand = ops::Visc::template run<GEO, P2>(c, 0, i, j, k, bad);
-            best = dev::pmin(best, cand);
+            if (half == 0)
+                ops::Visc::heat_forces<GEO, P2>(c, i, j, k, bad);
+            else if (i <= c.g.nx && j <= c.g.ny && k <= c.g.nz)
+                best = dev::pmin(best, ops::Visc::cfl<GEO, P2>(c, i, j, k, bad));
         }
     }
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c.sc->status, 1);
@@ -1276,17 +1284,19 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     }
     launch<ops::Alpha>(0);
     {
+        // Visc with two threads per cell (k_visc_split): 1.21 -> 1.12 ms at
+        // 256^3 against one thread per cell at 128 registers
         int lo[3], hi[3];
         ops::Visc::bounds(ctx_.g, 0, lo, hi);
         const long long plane = (long long)(hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
         const int ni = hi[0] - lo[0] + 1;
-        dim3 grid((unsigned)ceil_div(plane, kThreads), (unsigned)(ni < 16 ? ni : 16));
+        dim3 grid((unsigned)ceil_div(plane, kThreads / 2), (unsigned)(ni < 16 ? ni : 16));
         if (ctx_.p.geometry)
-            k_visc<true, false><<<grid, kThreads, 0, stream_>>>(ctx_);
+            k_visc_split<true, false><<<grid, kThreads, 0, stream_>>>(ctx_);
         else if (ctx_.p.pow2)
-            k_visc<false, true><<<grid, kThreads, 0, stream_>>>(ctx_);
+            k_visc_split<false, true><<<grid, kThreads, 0, stream_>>>(ctx_);
         else
-            k_visc<false, false><<<grid, kThreads, 0, stream_>>>(ctx_);
+            k_visc_split<false, false><<<grid, kThreads, 0, stream_>>>(ctx_);
         ++launches_;
     }
     if (halo_) halo_->reduce_dt(*this);
