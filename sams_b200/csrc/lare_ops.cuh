@@ -1291,9 +1291,13 @@ struct SweepCTMass {
         st.put(DB2, dba2);
     }
     // CT fluxes where `ct` ((i, j, k) in 0..n), the mass flux everywhere it
-    // is called (0..n along the sweep, 0..n+1 across)
+    // is called (0..n along the sweep, 0..n+1 across).  With `images` (dm
+    // periodic along the sweep, at least three cells) the mass flux also goes
+    // to the ghost points that the periodic fill along the sweep would copy it
+    // to (sweep index n-1, n -> -1, 0 and 1, 2 -> n+1, n+2), and index 0,
+    // which that fill overwrites, is left alone, so the fill is not needed.
     template <bool GEO, class A>
-    __device__ static void fluxes(const Ctx &c, int i, int j, int k, A st, bool ct)
+    __device__ static void fluxes(const Ctx &c, int i, int j, int k, A st, bool ct, bool images = false)
     {
         const Geom &g = c.g;
         const int o = LOFF(i, j, k);
@@ -1312,8 +1316,18 @@ struct SweepCTMass {
                                         st.get(F2, 2), st.get(DB2, 0), st.get(DB2, 1), dci, dcm, dcp, cvi, cvp);
         }
         const RO rho{c.f[SAMS_F_RHO]};
-        c.f[SAMS_F_DM][o] = mass_flux(face_velocity<DIR>(c, o), dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d],
-                                      rho[o], rho[o + d], rho[o + 2 * d], dci, dcm, dcp, cvi, cvp);
+        const double m = mass_flux(face_velocity<DIR>(c, o), dt, face_area<DIR, GEO>(c, i, j, k), rho[o - d],
+                                   rho[o], rho[o + d], rho[o + 2 * d], dci, dcm, dcp, cvi, cvp);
+        double *dm = c.f[SAMS_F_DM];
+        if (!images) {
+            dm[o] = m;
+            return;
+        }
+        const int s = DIR == 0 ? i : (DIR == 1 ? j : k);
+        const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+        if (s >= 1) dm[o] = m;
+        if (s >= nd - 1) dm[o - nd * d] = m;
+        if (s >= 1 && s <= 2) dm[o + nd * d] = m;
     }
 };
 

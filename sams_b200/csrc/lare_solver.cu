@@ -18,7 +18,7 @@
 //        of place, with SweepCTUpd), fill the nine state fields
 //     z: k_cellnode_march (SweepVol + SweepCvc), k_ctmass_z, fill dm along
 //        z, k_zsweep (S6-S8 in place, with SweepCTUpd bringing B back from
-//        flux form), fill the state fields but B, fill B
+//        flux form), fill the nine state fields
 // Other solves take the separate kernels (CellPrep, NodePrep, Corr1,
 // SweepVol, SweepCvc, BScale, SweepS6/S7/S8, the rke kernels, k_copy_shell) where a
 // condition above fails (thin grids, rke, a field edge without a condition).
@@ -440,7 +440,7 @@ struct CtStore {
 };
 
 template <int DIR, bool GEO>
-__global__ void __launch_bounds__(ops::kWinThreads, 5) k_ctmass(Ctx c, int scale)  // cap tuned on B200
+__global__ void __launch_bounds__(ops::kWinThreads, 5) k_ctmass(Ctx c, int scale, int images)  // cap tuned on B200
 {
     using F = ops::SweepCTMass<DIR>;
     constexpr int TK = ops::kWinK, TS = ops::kWinThreads / ops::kWinK;
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(ops::kWinThreads, 5) k_ctmass(Ctx c, int scale
     __syncthreads();
     if (mass)
         for (int s = s0 + sl; s <= s1; s += TS)
-            F::template fluxes<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), ct);
+            F::template fluxes<GEO>(c, DIR == 0 ? s : a, DIR == 0 ? a : s, k, at(s), ct, images != 0);
 }
 
 // SweepCT + SweepMass of the z sweep: kZRows lines (i, j) in 0..nx+1 x
@@ -477,7 +477,7 @@ struct ZRowStore {
 };
 
 template <bool GEO>
-__global__ void __launch_bounds__(256, 5) k_ctmass_z(Ctx c)  // cap tuned on B200
+__global__ void __launch_bounds__(256, 5) k_ctmass_z(Ctx c, int images)  // cap tuned on B200
 {
     using F = ops::SweepCTMass<2>;
     __shared__ double zsm[F::NARR * kZRows * kZSpan];
@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(256, 5) k_ctmass_z(Ctx c)  // cap tuned on B20
     __syncthreads();
     for (int kk = kc; kk < kZOwn; kk += 32) {
         const int k = k0 + kk;  // along the sweep: 0..nz for both fluxes
-        if (on && k <= g.nz) F::fluxes<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk + 1}, ct);
+        if (on && k <= g.nz) F::fluxes<GEO>(c, i, j, k, ZRowStore{zsm, r * kZSpan + kk + 1}, ct, images != 0);
     }
 }
 
@@ -1142,7 +1142,7 @@ void Solver::launch_resist(bool last)
 
 // SweepCT + SweepMass of one sweep (k_ctmass / k_ctmass_z).
 template <int DIR>
-void Solver::launch_ctmass(int scale)
+bool Solver::launch_ctmass(int scale)
 {
     const Geom &g = ctx_.g;
     // windows over k (x, y: kWinK lanes over 0..nz+1; z: kZOwn own k per
@@ -1151,26 +1151,32 @@ void Solver::launch_ctmass(int scale)
     if (!window) {  // (the solver folds the B scaling in only where the x window runs: scale == 0 here)
         launch<ops::SweepCT<DIR>>(0);
         launch<ops::SweepMass<DIR>>(0);
-        return;
+        return false;
     }
+    // dm's periodic fill along the sweep folded into the kernel (the slabs'
+    // x fill is an exchange between slabs and stays)
+    const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+    const int images = !(halo_ && DIR == 0) && nd >= kBcSequentialBelow &&
+                       bc_.kind[SAMS_F_DM][DIR][0] == SAMS_BC_PERIODIC && bc_.kind[SAMS_F_DM][DIR][1] == SAMS_BC_PERIODIC;
     if (DIR == 2) {
         const long long lines = (long long)(g.nx + 2) * (g.ny + 2);
         dim3 grid((unsigned)ceil_div(lines, kZRows), (unsigned)ceil_div(g.nz + 1, kZOwn));
         if (ctx_.p.geometry)
-            k_ctmass_z<true><<<grid, 256, 0, stream_>>>(ctx_);
+            k_ctmass_z<true><<<grid, 256, 0, stream_>>>(ctx_, images);
         else
-            k_ctmass_z<false><<<grid, 256, 0, stream_>>>(ctx_);
+            k_ctmass_z<false><<<grid, 256, 0, stream_>>>(ctx_, images);
     } else {
-        const int nd = DIR == 0 ? g.nx : g.ny, na = DIR == 0 ? g.ny : g.nx;
+        const int na = DIR == 0 ? g.ny : g.nx;
         const long long blocks = (long long)(na + 2) * ((g.nz + 1 + ops::kWinK) / ops::kWinK) *
                                  ((nd + kCtS) / kCtS);
         const size_t smem = (size_t)ops::SweepCTMass<DIR>::NARR * kCtP * ops::kWinK * sizeof(double);
         if (ctx_.p.geometry)
-            k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale);
+            k_ctmass<DIR, true><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale, images);
         else
-            k_ctmass<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale);
+            k_ctmass<DIR, false><<<(unsigned)blocks, ops::kWinThreads, smem, stream_>>>(ctx_, scale, images);
     }
     ++launches_;
+    return images != 0;
 }
 
 template <class Op>
@@ -1349,7 +1355,7 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepVol<0>>(!p_.rke && psweep_ok_ ? 1 : 0);
         launch<ops::SweepCvc>(0);
     }
-    launch_ctmass<0>(b_fill_all ? 1 : 0);
+    const bool dm_x = launch_ctmass<0>(b_fill_all ? 1 : 0);
     // The CT update changes only B, which the dm fill and the stages S6-S8
     // do not read, so the y and z sweeps' fused stages take it at their
     // points 0..n (its whole range).  In the x sweep, with the B scaling
@@ -1358,7 +1364,7 @@ void Solver::enqueue_step(cudaEvent_t *marks)
     // 40 us).
     const bool fused_xy = !p_.rke && psweep_ok_;  // k_psweep runs the x and y stages
     launch<ops::SweepCTUpd<0>>(b_fill_all ? 1 : 0);
-    bc_fill_dim(FM_DM, 0);
+    if (!dm_x) bc_fill_dim(FM_DM, 0);
     if (fused_xy) {
         launch_psweep<0>(-1);
     } else {
@@ -1378,9 +1384,9 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepVol<1>>(!p_.rke && psweep_ok_ ? 1 : 0);
         launch<ops::SweepCvc>(0);
     }
-    launch_ctmass<1>(0);
+    const bool dm_y = launch_ctmass<1>(0);
     if (!fused_xy) launch<ops::SweepCTUpd<1>>(0);
-    bc_fill_dim(FM_DM, 1);
+    if (!dm_y) bc_fill_dim(FM_DM, 1);
     if (fused_xy) {
         launch_psweep<1>(0);
     } else {
@@ -1400,10 +1406,10 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         launch<ops::SweepVol<2>>(0);
         launch<ops::SweepCvc>(0);
     }
-    launch_ctmass<2>(0);
+    const bool dm_z = launch_ctmass<2>(0);
     const bool zfused = !p_.rke && ctx_.g.nz + 4 <= kZThreads;
     if (!zfused) launch<ops::SweepCTUpd<2>>(b_fill_all ? 2 : 0);
-    bc_fill_dim(FM_DM, 2);
+    if (!dm_z) bc_fill_dim(FM_DM, 2);
     if (zfused) {
         const Geom &g = ctx_.g;
         const int W = g.nz + 4, lines = kZThreads / W;
@@ -1425,9 +1431,14 @@ void Solver::enqueue_step(cudaEvent_t *marks)
         }
         launch<ops::SweepS8<2>>(0);
     }
-    bc_fill(b_fill_all ? FM_ALL9 & ~FM_BFIELD : FM_ALL9);
-    if (!b_fill_all) launch<ops::BScale>(1);
-    bc_fill(FM_BFIELD);
+    // with the B scaling folded into the z sweep's CT update, B needs no pass
+    // of its own before the fill, so all nine fields take one fill (the fill
+    // of each field is independent of the others')
+    bc_fill(FM_ALL9);
+    if (!b_fill_all) {
+        launch<ops::BScale>(1);
+        bc_fill(FM_BFIELD);
+    }
     if (p_.rke) launch<ops::RkeEnergy>(0);  // after the remap (shared_data.h:414-417)
     mark(5);
 }

@@ -115,7 +115,8 @@ private:
     template <class P> void launch_edges();
     void launch_pred(int resistive);
     void launch_resist(bool last);
-    template <int DIR> void launch_ctmass(int scale);
+    // true when the kernel also wrote dm's periodic ghost images along DIR
+    template <int DIR> bool launch_ctmass(int scale);
     int setup_psweep();
     int staging(double **out);
     void free_all();
