@@ -91,3 +91,22 @@ def test_harris_pressure_balance():
     rho, ee, ei, bx = f[0][2:-2, 2:-2, 2:-2], f[1][2:-2, 2:-2, 2:-2], f[2][2:-2, 2:-2, 2:-2], f[9][2:-2, 2:-2, 2:-2]
     ptot = (g - 1) * rho * (ee + ei) + 0.5 * bx ** 2
     assert np.allclose(ptot, 0.55, rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("n,own_stream", [((32, 32, 32), False), ((64, 64, 64), False), ((96, 96, 96), True),
+                                          ((192, 192, 192), True), ((256, 256, 4), False), ((20, 16, 24), True)])
+def test_serve_footprint_follows_the_path_a_solve_takes(n, own_stream):
+    """The server charges a solve the device bytes of the path it runs on:
+    its own solver (padded rows, 32 arrays, host-transfer staging) when its
+    z lines fill the fused kernels' tiles (nz >= 23 with full tiles), else a
+    batch slot (dense rows).  Host arithmetic only, no GPU."""
+    p, _ = lare.case_setup("rf", *n)
+    got = lare.solve_bytes(p)
+    nx, ny, nz = n
+    zrow = (nz + 6 + 7) // 8 * 8
+    solver = (32 * (nx + 5) * (ny + 5) * zrow + (nx + 5) * (ny + 5) * (nz + 5) + 6 * (nx + ny + nz + 18)) * 8
+    batch_arrays = 32 * (nx + 5) * (ny + 5) * (nz + 5) * 8
+    if own_stream:
+        assert solver <= got <= solver + 8192
+    else:
+        assert batch_arrays <= got < solver
