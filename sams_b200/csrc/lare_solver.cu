@@ -148,7 +148,6 @@ constexpr int kRP = (kMK + 1) * (kMJ + 1);  // cells of one ring plane
 constexpr int kMThreads = (kRP + 31) / 32 * 32;
 
 struct RingSrc {
-    static constexpr bool kPressureSum = false;
     const double *ring;
     __device__ double operator()(int arr, int q) const { return ring[arr * 3 * kRP + q]; }
 };
