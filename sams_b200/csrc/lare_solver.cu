@@ -527,8 +527,8 @@ __global__ void __launch_bounds__(kThreads) k_copy_shell(Ctx c, ops::SweepOut w)
     }
 }
 
-// Visc with two threads per cell: a block holds 128 cells of a plane row,
-// its first four warps run the viscous heating and forces
+// Visc with two threads per cell: a block holds 128 consecutive (j, k)
+// points of a y-z plane (walking i); its first four warps run the viscous heating and forces
 // (ops::Visc::heat_forces), the other four the viscous pressure and CFL
 // candidate (ops::Visc::cfl), so each thread carries half the work's live
 // values.  Both halves read the same corners, which the block's L1 serves.
